@@ -1,0 +1,233 @@
+/*
+ * monkeygl_b200.h -- C ABI of the B200 (sm_100a) volume ray-casting library.
+ *
+ * This is the seam between host code (the C++ HelloMonkey/IRender API, the
+ * pyMonkeyGL module, ctypes callers) and the hand-written CUDA kernels.  Every
+ * entry point takes plain pointers, sizes and POD structs; nothing here needs
+ * CUDA or torch headers.  Each declaration names the MonkeyGL interface it
+ * replaces (paths relative to the MonkeyGL source tree).
+ *
+ * Conventions
+ *   - Every function returns an mk_status (0 = MK_OK).  No entry point exits
+ *     the process; CUDA errors come back as MK_ERR_CUDA and the text of the
+ *     last error is available from mk_last_error().
+ *   - Volumes are x-fastest int16 arrays (dim_x * dim_y * dim_z), exactly the
+ *     buffer MonkeyGL's SetVolumeData takes (core/VolumeInfo.cpp:78-91).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the library's own
+ *     per-volume stream).  Calls with host output pointers are synchronous with
+ *     respect to that stream; calls with device output pointers are
+ *     asynchronous.
+ *   - Outputs are caller-owned.  The library allocates device memory only at
+ *     volume creation and when an output larger than any before is requested.
+ */
+#ifndef MONKEYGL_B200_H
+#define MONKEYGL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Labels 0..64: MAXOBJECTCOUNT + 1 (core/Defines.h:34). */
+#define MK_MAX_LABELS 65
+
+typedef enum mk_status {
+    MK_OK = 0,
+    MK_ERR_INVALID_ARGUMENT = 1,
+    MK_ERR_CUDA = 2,
+    MK_ERR_OUT_OF_MEMORY = 3,
+    MK_ERR_NOT_READY = 4,
+    MK_ERR_BUDGET = 5,
+    MK_ERR_TIMEOUT = 6,
+    MK_ERR_NO_DEVICE = 7,
+    MK_ERR_QUEUE_FULL = 8
+} mk_status;
+
+/* RenderType (core/Defines.h:224-230). */
+typedef enum mk_render_type {
+    MK_RENDER_VR = 0,
+    MK_RENDER_MIP = 1,
+    MK_RENDER_SURFACE = 2
+} mk_render_type;
+
+/* MPRType (core/Defines.h:216-222). */
+typedef enum mk_mpr_type {
+    MK_MPR_AVERAGE = 0,
+    MK_MPR_MIP = 1,
+    MK_MPR_MINIP = 2
+} mk_mpr_type;
+
+/* Volume sampling for planes.  MonkeyGL only has LINEAR (its texture is
+ * created with cudaFilterModeLinear, core/CuDataManager.cu:64); NEAREST is the
+ * same reslice read through a point-filtered view of the same voxels. */
+typedef enum mk_sampling {
+    MK_SAMPLE_LINEAR = 0,
+    MK_SAMPLE_NEAREST = 1
+} mk_sampling;
+
+/* VR output pixel layout.  MonkeyGL returns 3 bytes per pixel, R,G,B
+ * (core/kernel.cu:258-262); RGBA8 is the same colour with A = 255. */
+typedef enum mk_pixel_format {
+    MK_PIXEL_RGB8 = 0,
+    MK_PIXEL_RGBA8 = 1
+} mk_pixel_format;
+
+/* mk_vr_params.flags */
+#define MK_VR_NO_SKIP 0x1 /* march every reference sample (no empty-space skipping) */
+
+typedef struct mk_volume_s *mk_volume;
+
+/*
+ * Ray-casting parameters: the scalar arguments of MonkeyGL's cu_render
+ * (core/kernel.cu:471-492), in the same meaning and units.
+ */
+typedef struct mk_vr_params {
+    int width;
+    int height;
+    int render_type;             /* mk_render_type */
+    float max_len_spacing[3];    /* f3maxLenSpacing (core/DataManager.h:201-216) */
+    float spacing[3];            /* f3Spacing */
+    float spacing_voxel[3];      /* f3SpacingVoxel = 1/dim */
+    float x_translate;           /* RenderInfo total pan, pixels */
+    float y_translate;
+    float scale;                 /* RenderInfo total zoom */
+    float transform[9];          /* row-major 3x3 camera matrix (float3x3 m[3]) */
+    int invert_z;
+    int voi[6];                  /* left, right, posterior, anterior, head, foot */
+    float background[4];         /* RGBA background, used only where nothing composited */
+    int pixel_format;            /* mk_pixel_format */
+    int flags;                   /* MK_VR_* */
+} mk_vr_params;
+
+/*
+ * MPR parameters: the arguments of cu_renderPlane_{Average,MIP,MinIP}
+ * (core/kernel.cu:616-631, 706-721, 795-810), plus the reslice mode.
+ */
+typedef struct mk_plane_params {
+    int width;
+    int height;
+    int mpr_type;                /* mk_mpr_type */
+    int sampling;                /* mk_sampling */
+    float spacing[3];            /* voxel spacing, mm */
+    float dir_h[3];              /* unit row direction */
+    float dir_v[3];              /* unit column direction */
+    float dir_n[3];              /* unit slab normal */
+    float left_top[3];           /* plane corner, mm from the volume corner */
+    float pixel_spacing;         /* mm per output pixel */
+    int invert_z;
+    float half_num;              /* slab half width in samples: (n - 1) / 2 */
+} mk_plane_params;
+
+/* ------------------------------------------------------------------ */
+/* Library / device                                                    */
+/* ------------------------------------------------------------------ */
+
+/* Text for a status code. */
+const char *mk_status_string(int status);
+/* Text of the last error recorded on the calling thread ("" if none). */
+const char *mk_last_error(void);
+/* Number of visible CUDA devices (0 when none).  Replaces DeviceInfo::GetCount
+ * (core/DeviceInfo.cpp:91-97). */
+int mk_device_count(int *count);
+/* Library version string, "major.minor.patch". */
+const char *mk_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Volume residency                                                    */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Upload an int16 volume to `device` and build its brick occupancy map.
+ * Replaces cu_copyVolumeData (core/CuDataManager.cu:28-73).  The host buffer
+ * may be freed after the call returns.
+ */
+int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x, int dim_y,
+                     int dim_z, int device);
+/* Release every device resource of the volume. */
+int mk_volume_destroy(mk_volume vol);
+/* Device bytes held by the volume (textures, maps, buffers). */
+int mk_volume_device_bytes(mk_volume vol, size_t *bytes);
+/* Dimensions of the volume. */
+int mk_volume_dims(mk_volume vol, int *dim_x, int *dim_y, int *dim_z);
+
+/*
+ * Upload (labels != NULL) or remove (labels == NULL) the uint8 label volume,
+ * same dims and layout as the voxels.  Replaces cu_copyMaskData
+ * (core/CuDataManager.cu:75-120).
+ */
+int mk_volume_set_mask(mk_volume vol, const uint8_t *labels);
+
+/*
+ * Set the RGBA lookup table of one label: `n_entries` float4 (r,g,b,a) in
+ * [0,1], filtered linearly over t in [0,1] with entry centres at (i+0.5)/n.
+ * Replaces cu_setTransferFunc (core/CuDataManager.cu:122-163).  A label with
+ * no table renders as fully transparent.
+ */
+int mk_volume_set_transfer_function(mk_volume vol, int label, const float *rgba,
+                                    int n_entries);
+
+/*
+ * Per-label opacity cap, window width and window level: `n_labels` rows of
+ * (alpha, ww, wl).  Replaces the AlphaAndWWWLInfo argument of cu_render
+ * (core/Defines.h:123-149, core/DataManager.cpp:602-611).  ww must be > 0.
+ */
+int mk_volume_set_label_params(mk_volume vol, const float *alpha_ww_wl, int n_labels);
+
+/* ------------------------------------------------------------------ */
+/* Rendering                                                           */
+/* ------------------------------------------------------------------ */
+
+/*
+ * Ray-cast the volume (VR, MIP or first-hit surface) into an image of
+ * width*height pixels, 3 (RGB8) or 4 (RGBA8) bytes each, row-major.
+ * Replaces cu_render (core/kernel.cu:471-568).  `out` is host memory when
+ * out_on_device == 0 (the call then returns with the image in `out`), else a
+ * device pointer (the call returns after queuing the work on `stream`).
+ */
+int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out,
+                 int out_on_device, void *stream);
+
+/*
+ * Count the samples of MonkeyGL's own ray schedule for this frame (positions
+ * inside the volume where its d_render/d_renderMIP/d_renderSurface would
+ * fetch a voxel, core/kernel.cu:195-252, 311-349, 413-453).  This is the unit
+ * of the Gsamples/s figure; it does not render.
+ */
+int mk_count_vr_samples(mk_volume vol, const mk_vr_params *params, uint64_t *samples);
+
+/*
+ * Reslice a plane (MPR) into width*height int16 values.  Replaces
+ * cu_renderPlane_{Average,MIP,MinIP} (core/kernel.cu:570-837).
+ */
+int mk_render_plane(mk_volume vol, const mk_plane_params *params, int16_t *out,
+                    int out_on_device, void *stream);
+
+/*
+ * Optional display epilogue for planes: window/level the int16 plane into
+ * uint8 (0 below wl - ww/2, 255 above wl + ww/2, linear between).  MonkeyGL
+ * applies this in its HTML client (cornerstone windowing set up in
+ * examples/html/js/utils.js:40-60).
+ */
+int mk_render_plane_u8(mk_volume vol, const mk_plane_params *params, float ww, float wl,
+                       uint8_t *out, int out_on_device, void *stream);
+
+/*
+ * Curved planar reformation: row y samples points[y] + x * dirs[y] (voxel
+ * units, x = 0..width-1); out-of-volume pixels are -2048.  `points` and
+ * `dirs` are height*3 doubles each, as built by CPRInfo (core/CPRInfo.cpp:81-160).
+ * Replaces cu_renderCPR (core/kernel.cu:839-918).
+ */
+int mk_render_cpr(mk_volume vol, int width, int height, const double *points,
+                  const double *dirs, int invert_z, int16_t *out, int out_on_device,
+                  void *stream);
+
+/* Wait for all work queued on `stream` (NULL = the volume's stream). */
+int mk_volume_synchronize(mk_volume vol, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MONKEYGL_B200_H */

@@ -1,0 +1,115 @@
+// mk_internal.h -- device-side state of a resident volume and the parameter
+// blocks the kernels receive.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/monkeygl_b200.h"
+
+namespace mk {
+
+// Bricks are 8^3 voxels.  A brick "owns" the sample positions whose integer
+// voxel index (trunc(pos * dim), core/kernel.cu:208-210) falls inside it; its
+// value footprint is the owned voxels plus a one-voxel apron, which covers
+// every trilinear tap of an owned sample.
+constexpr int kBrickShift = 3;
+constexpr int kBrick = 1 << kBrickShift;
+
+// Transfer-function alpha at or below this bound counts as empty.  MonkeyGL
+// composites only samples with alpha > 0.0005 and refines the step only for
+// alpha > 0.001 (core/kernel.cu:101, 242); the margin absorbs the rounding of
+// the linear LUT filter.
+constexpr float kEmptyAlpha = 0.0004f;
+
+// Labels whose opacity cap needs a running per-ray accumulator, tracked in
+// shared memory; volumes with more such labels use the local-memory path.
+constexpr int kMaxTrackedLabels = 16;
+
+struct LabelTable {
+    cudaTextureObject_t tf[MK_MAX_LABELS];   // 0 = no table (transparent)
+    float alpha[MK_MAX_LABELS];
+    float ww[MK_MAX_LABELS];
+    float wl[MK_MAX_LABELS];
+};
+
+// Per-frame view of the brick maps handed to the ray-casting kernels.
+struct BrickView {
+    const uint32_t *visible_bits;   // VR: 1 = some sample may have alpha > kEmptyAlpha
+    const float *mip_tmax;          // MIP: upper bound of the windowed value over labels with alpha > 0
+    const short2 *minmax;           // raw voxel min/max of the footprint
+    int nbx, nby, nbz;
+};
+
+struct VolumeState {
+    int device = 0;
+    int dims[3] = {0, 0, 0};
+    cudaStream_t stream = nullptr;
+
+    cudaArray_t vol_array = nullptr;
+    cudaTextureObject_t tex_linear = 0;   // normalized coords, trilinear, clamp, normalized float
+    cudaTextureObject_t tex_point = 0;    // same array, nearest
+    cudaArray_t mask_array = nullptr;
+    cudaTextureObject_t tex_mask = 0;     // unnormalized coords, nearest, element type
+
+    cudaArray_t tf_array[MK_MAX_LABELS] = {};
+    cudaTextureObject_t tf_tex[MK_MAX_LABELS] = {};
+    float *d_tf_alpha[MK_MAX_LABELS] = {};   // LUT alpha column, for the visibility pass
+    int tf_len[MK_MAX_LABELS] = {};
+    float params[MK_MAX_LABELS][3];          // alpha, ww, wl
+
+    // brick maps
+    int nb[3] = {0, 0, 0};
+    short2 *d_minmax = nullptr;
+    uint32_t *d_labels = nullptr;            // 3 words (labels 0..64) per brick
+    uint32_t *d_visible = nullptr;           // 1 bit per brick
+    float *d_mip_tmax = nullptr;
+    bool maps_dirty = true;
+    uint64_t present_labels[2] = {1, 0};     // labels occurring anywhere in the mask
+
+    // ray schedule: accuLength after k plain steps of 1/dim_z
+    float *d_accu = nullptr;
+    int accu_len = 0;
+
+    // output staging
+    void *d_out = nullptr;
+    size_t d_out_bytes = 0;
+    void *h_pinned = nullptr;
+    size_t h_pinned_bytes = 0;
+    unsigned long long *d_counter = nullptr;
+
+    size_t device_bytes = 0;
+};
+
+// Thread-local last-error text (set by the C ABI on failure).
+void set_last_error(const std::string &msg);
+
+#define MK_CUDA_TRY(expr)                                                        \
+    do {                                                                         \
+        cudaError_t _e = (expr);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            ::mk::set_last_error(std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+            return (_e == cudaErrorMemoryAllocation) ? MK_ERR_OUT_OF_MEMORY      \
+                                                     : MK_ERR_CUDA;              \
+        }                                                                        \
+    } while (0)
+
+// Smallest float strictly greater than the double bound c; for a float a,
+// a < c  <=>  a < float_bound_above(c) when c is not itself a float.
+float float_bound_above(double c);
+
+// Host helpers shared by the entry points.
+int ensure_device_buffer(VolumeState *v, size_t bytes);
+int ensure_pinned_buffer(VolumeState *v, size_t bytes);
+int rebuild_brick_maps(VolumeState *v, cudaStream_t s);
+int finish_output(VolumeState *v, void *out, size_t bytes, int out_on_device, cudaStream_t s);
+BrickView brick_view(const VolumeState *v);
+LabelTable label_table(const VolumeState *v);
+
+}  // namespace mk
+
+struct mk_volume_s {
+    mk::VolumeState st;
+};

@@ -1,0 +1,251 @@
+// mk_reslice.cu -- planar (MPR) and curved (CPR) reslicing of a resident
+// volume into int16 images.
+//
+// Method: MonkeyGL's d_renderPlane_{MIP,MinIP,Average} and d_renderCPR
+// (core/kernel.cu:570-873): each output pixel maps to a point in volume
+// millimetres (planes) or voxel units (CPR), is normalised by the volume
+// extent, z-flipped unless the volume is already inverted, and read through
+// the trilinear texture scaled by 32768; slabs reduce 2*halfNum+1 samples
+// along the plane normal by max, min or mean.  The coordinate expressions keep
+// MonkeyGL's operation order; its FP64 pieces (the CPR point arithmetic and
+// the slab-mean accumulator) are evaluated with error-free FP32 pairs
+// (mk_math.h).  MK_SAMPLE_NEAREST reads the same voxels through a
+// point-filtered texture view.
+//
+// Layout: 256-thread blocks cover 32x8 output tiles so each warp stores one
+// 64-byte row segment; CPR rows share their (point, direction) pair through
+// shared memory.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "mk_internal.h"
+#include "mk_math.h"
+
+namespace mk {
+
+struct PlaneParams {
+    int W, H;
+    float sp[3];
+    float fdim[3];
+    float h[3], v[3], n[3], lt[3];
+    float ps;
+    int invertZ;
+    float halfNum;
+    int mode;
+    float ww, wl;      // u8 epilogue
+};
+
+template <int MODE>
+__device__ __forceinline__ short reslice_pixel(const PlaneParams &P, cudaTextureObject_t tex, int x,
+                                               int y) {
+    short acc = (MODE == MK_MPR_MIP) ? (short)-32768 : (short)32767;
+    fsum sum = {0.0f, 0.0f};
+    for (float t = -P.halfNum; t <= P.halfNum; t += 1) {
+        const float fLength = t * P.ps;
+        const float pt_x = P.lt[0] + fLength * P.n[0];
+        const float pt_y = P.lt[1] + fLength * P.n[1];
+        const float pt_z = P.lt[2] + fLength * P.n[2];
+        const float fx = (pt_x + x * P.ps * P.h[0] + y * P.ps * P.v[0]) / (P.sp[0] * P.fdim[0]);
+        const float fy = (pt_y + x * P.ps * P.h[1] + y * P.ps * P.v[1]) / (P.sp[1] * P.fdim[1]);
+        float fz = (pt_z + x * P.ps * P.h[2] + y * P.ps * P.v[2]) / (P.sp[2] * P.fdim[2]);
+        // "fz = 1.0 - fz" in double, then rounded to float: identical to the
+        // float subtraction for every float fz (the exact difference rounds once)
+        if (!P.invertZ) fz = 1.0f - fz;
+        const bool inside = fx >= 0 && fx <= 1 && fy >= 0 && fy <= 1 && fz >= 0 && fz <= 1;
+        if (MODE == MK_MPR_AVERAGE) {
+            fsum_add(sum, inside ? 32768 * tex3D<float>(tex, fx, fy, fz) : -32768.0f);
+        } else {
+            const short val = inside ? f2s_sat(32768 * tex3D<float>(tex, fx, fy, fz)) : (short)-32768;
+            if (MODE == MK_MPR_MIP) acc = acc > val ? acc : val;
+            else acc = acc < val ? acc : val;
+        }
+    }
+    if (MODE == MK_MPR_AVERAGE) return fsum_div_to_short(sum, 2 * P.halfNum + 1);
+    return acc;
+}
+
+template <int MODE, bool U8>
+__global__ void __launch_bounds__(256) k_plane(PlaneParams P, cudaTextureObject_t tex, void *out) {
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= P.W || y >= P.H) return;
+    const short r = reslice_pixel<MODE>(P, tex, x, y);
+    if (U8) {
+        // linear window: 0 at wl - ww/2, 255 at wl + ww/2
+        float g = ((float)r - (P.wl - 0.5f * P.ww)) / P.ww * 255.0f;
+        g = fminf(fmaxf(g, 0.0f), 255.0f);
+        static_cast<uint8_t *>(out)[(size_t)y * P.W + x] = (uint8_t)(g + 0.5f);
+    } else {
+        static_cast<short *>(out)[(size_t)y * P.W + x] = r;
+    }
+}
+
+// CPR row data: the double point / direction of each row as float pairs.
+struct CprRow {
+    float p_hi[3], p_lo[3], d_hi[3], d_lo[3];
+};
+
+__global__ void __launch_bounds__(256) k_cpr(int W, int H, float3 fdim, int invertZ,
+                                             const CprRow *__restrict__ rows,
+                                             cudaTextureObject_t tex, short *out) {
+    __shared__ CprRow s_rows[8];
+    const int ly = threadIdx.x >> 5;
+    const int y = blockIdx.y * 8 + ly;
+    if ((threadIdx.x & 31) == 0 && y < H) s_rows[ly] = rows[y];
+    __syncthreads();
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    if (x >= W || y >= H) return;
+    const CprRow &R = s_rows[ly];
+    const float xf = (float)x;
+    const float fx = cpr_coord(R.p_hi[0], R.p_lo[0], R.d_hi[0], R.d_lo[0], xf, fdim.x);
+    const float fy = cpr_coord(R.p_hi[1], R.p_lo[1], R.d_hi[1], R.d_lo[1], xf, fdim.y);
+    float fz = cpr_coord(R.p_hi[2], R.p_lo[2], R.d_hi[2], R.d_lo[2], xf, fdim.z);
+    if (!invertZ) fz = 1.0f - fz;
+    short r;
+    if (fx < 0 || fx > 1 || fy < 0 || fy > 1 || fz < 0 || fz > 1) r = -2048;
+    else r = f2s_sat(32768 * tex3D<float>(tex, fx, fy, fz));
+    out[(size_t)y * W + x] = r;
+}
+
+static int fill_plane(const VolumeState &v, const mk_plane_params *p, PlaneParams &P) {
+    if (!p || p->width <= 0 || p->height <= 0 || p->width > 32768 || p->height > 32768) {
+        set_last_error("mk_render_plane: plane size must be in [1, 32768]");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (p->mpr_type < MK_MPR_AVERAGE || p->mpr_type > MK_MPR_MINIP ||
+        (p->sampling != MK_SAMPLE_LINEAR && p->sampling != MK_SAMPLE_NEAREST)) {
+        set_last_error("mk_render_plane: unknown MPR type or sampling");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (!(p->half_num >= 0.0f) || p->half_num > 4096.0f) {
+        set_last_error("mk_render_plane: half_num must be in [0, 4096]");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    P.W = p->width;
+    P.H = p->height;
+    for (int k = 0; k < 3; ++k) {
+        P.sp[k] = p->spacing[k];
+        P.fdim[k] = (float)v.dims[k];
+        P.h[k] = p->dir_h[k];
+        P.v[k] = p->dir_v[k];
+        P.n[k] = p->dir_n[k];
+        P.lt[k] = p->left_top[k];
+    }
+    P.ps = p->pixel_spacing;
+    P.invertZ = p->invert_z ? 1 : 0;
+    P.halfNum = p->half_num;
+    P.mode = p->mpr_type;
+    P.ww = 1.0f;
+    P.wl = 0.0f;
+    return MK_OK;
+}
+
+template <bool U8>
+static void launch_plane(const PlaneParams &P, cudaTextureObject_t tex, void *out, cudaStream_t s) {
+    dim3 grid((P.W + 31) / 32, (P.H + 7) / 8);
+    if (P.mode == MK_MPR_AVERAGE) k_plane<MK_MPR_AVERAGE, U8><<<grid, 256, 0, s>>>(P, tex, out);
+    else if (P.mode == MK_MPR_MIP) k_plane<MK_MPR_MIP, U8><<<grid, 256, 0, s>>>(P, tex, out);
+    else k_plane<MK_MPR_MINIP, U8><<<grid, 256, 0, s>>>(P, tex, out);
+}
+
+}  // namespace mk
+
+using namespace mk;
+
+extern "C" int mk_render_plane(mk_volume vol, const mk_plane_params *params, int16_t *out,
+                               int out_on_device, void *stream) {
+    if (!vol || !out) {
+        set_last_error("mk_render_plane: null volume or output");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &v = vol->st;
+    PlaneParams P;
+    int rc = fill_plane(v, params, P);
+    if (rc != MK_OK) return rc;
+    cudaSetDevice(v.device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
+    const size_t bytes = (size_t)P.W * P.H * sizeof(short);
+    void *dst = out;
+    if (!out_on_device) {
+        rc = ensure_device_buffer(&v, bytes);
+        if (rc != MK_OK) return rc;
+        dst = v.d_out;
+    }
+    const cudaTextureObject_t tex = params->sampling == MK_SAMPLE_NEAREST ? v.tex_point : v.tex_linear;
+    launch_plane<false>(P, tex, dst, s);
+    MK_CUDA_TRY(cudaGetLastError());
+    return finish_output(&v, out, bytes, out_on_device, s);
+}
+
+extern "C" int mk_render_plane_u8(mk_volume vol, const mk_plane_params *params, float ww, float wl,
+                                  uint8_t *out, int out_on_device, void *stream) {
+    if (!vol || !out || !(ww > 0.0f)) {
+        set_last_error("mk_render_plane_u8: null volume/output or ww <= 0");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &v = vol->st;
+    PlaneParams P;
+    int rc = fill_plane(v, params, P);
+    if (rc != MK_OK) return rc;
+    P.ww = ww;
+    P.wl = wl;
+    cudaSetDevice(v.device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
+    const size_t bytes = (size_t)P.W * P.H;
+    void *dst = out;
+    if (!out_on_device) {
+        rc = ensure_device_buffer(&v, bytes);
+        if (rc != MK_OK) return rc;
+        dst = v.d_out;
+    }
+    const cudaTextureObject_t tex = params->sampling == MK_SAMPLE_NEAREST ? v.tex_point : v.tex_linear;
+    launch_plane<true>(P, tex, dst, s);
+    MK_CUDA_TRY(cudaGetLastError());
+    return finish_output(&v, out, bytes, out_on_device, s);
+}
+
+extern "C" int mk_render_cpr(mk_volume vol, int width, int height, const double *points,
+                             const double *dirs, int invert_z, int16_t *out, int out_on_device,
+                             void *stream) {
+    if (!vol || !out || !points || !dirs || width <= 0 || height <= 0 || width > 32768 ||
+        height > 32768) {
+        set_last_error("mk_render_cpr: bad arguments");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &v = vol->st;
+    cudaSetDevice(v.device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
+    std::vector<CprRow> rows(height);
+    for (int y = 0; y < height; ++y) {
+        for (int k = 0; k < 3; ++k) {
+            const double p = points[3 * y + k], d = dirs[3 * y + k];
+            rows[y].p_hi[k] = (float)p;
+            rows[y].p_lo[k] = (float)(p - (double)rows[y].p_hi[k]);
+            rows[y].d_hi[k] = (float)d;
+            rows[y].d_lo[k] = (float)(d - (double)rows[y].d_hi[k]);
+        }
+    }
+    const size_t out_bytes = (size_t)width * height * sizeof(short);
+    const size_t row_bytes = (size_t)height * sizeof(CprRow);
+    const size_t row_off = (out_bytes + 255) & ~(size_t)255;
+    int rc = ensure_device_buffer(&v, row_off + row_bytes);
+    if (rc != MK_OK) return rc;
+    CprRow *d_rows = reinterpret_cast<CprRow *>(static_cast<char *>(v.d_out) + row_off);
+    rc = ensure_pinned_buffer(&v, row_bytes);
+    if (rc != MK_OK) return rc;
+    memcpy(v.h_pinned, rows.data(), row_bytes);
+    MK_CUDA_TRY(cudaMemcpyAsync(d_rows, v.h_pinned, row_bytes, cudaMemcpyHostToDevice, s));
+    short *dst = out_on_device ? out : static_cast<short *>(v.d_out);
+    dim3 grid((width + 31) / 32, (height + 7) / 8);
+    const float3 fdim = make_float3((float)v.dims[0], (float)v.dims[1], (float)v.dims[2]);
+    k_cpr<<<grid, 256, 0, s>>>(width, height, fdim, invert_z ? 1 : 0, d_rows, v.tex_linear, dst);
+    MK_CUDA_TRY(cudaGetLastError());
+    if (out_on_device) {
+        // the row table in the staging buffer must outlive the kernel
+        MK_CUDA_TRY(cudaStreamSynchronize(s));
+        return MK_OK;
+    }
+    return finish_output(&v, out, out_bytes, 0, s);
+}

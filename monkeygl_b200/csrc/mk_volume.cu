@@ -1,0 +1,665 @@
+// mk_volume.cu -- resident volumes: voxel texture, label texture, transfer
+// function tables, per-label parameters and the brick occupancy maps used
+// for empty-space skipping.
+//
+// Residency follows MonkeyGL's CuDataManager (core/CuDataManager.cu:28-163):
+// the int16 voxels live in a 3D cudaArray (block-linear, i.e. the hardware's
+// own 3D tiling) read through a normalized-coordinate, trilinear, clamped,
+// normalized-float texture; labels live in a uint8 cudaArray read with
+// nearest filtering at integer coordinates; each label's RGBA LUT is a 1D
+// float4 array read with linear filtering.  On top of that this file keeps,
+// per 8^3 brick, the voxel min/max over the brick's trilinear footprint and
+// the set of labels it owns, and rebuilds a visibility bitmap whenever a
+// transfer function or window changes.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <vector>
+
+#include "mk_internal.h"
+
+namespace mk {
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// One block per brick: min/max of the int16 voxels in the brick grown by one
+// voxel on every side (clamped to the volume), i.e. every voxel a trilinear
+// tap of an owned sample can touch.
+__global__ void __launch_bounds__(256) k_brick_minmax(const short *__restrict__ vox, int dx, int dy,
+                                                      int dz, int nbx, int nby, short2 *out) {
+    const int b = blockIdx.x;
+    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+    const int x0 = max(bx * kBrick - 1, 0), x1 = min(bx * kBrick + kBrick, dx - 1);
+    const int y0 = max(by * kBrick - 1, 0), y1 = min(by * kBrick + kBrick, dy - 1);
+    const int z0 = max(bz * kBrick - 1, 0), z1 = min(bz * kBrick + kBrick, dz - 1);
+    const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+    const int total = nx * ny * nz;
+    int lo = 32767, hi = -32768;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        int x = x0 + i % nx;
+        int y = y0 + (i / nx) % ny;
+        int z = z0 + i / (nx * ny);
+        int v = vox[((size_t)z * dy + y) * dx + x];
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    __shared__ int s_lo[8], s_hi[8];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        s_lo[w] = lo;
+        s_hi[w] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+            lo = min(lo, s_lo[i]);
+            hi = max(hi, s_hi[i]);
+        }
+        out[b] = make_short2((short)lo, (short)hi);
+    }
+}
+
+// One block per brick: the set of labels among the brick's owned voxels, as
+// a 65-bit mask in three words.
+__global__ void __launch_bounds__(256) k_brick_labels(const unsigned char *__restrict__ lab, int dx,
+                                                      int dy, int dz, int nbx, int nby,
+                                                      uint32_t *out) {
+    const int b = blockIdx.x;
+    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+    const int x0 = bx * kBrick, x1 = min(x0 + kBrick, dx) - 1;
+    const int y0 = by * kBrick, y1 = min(y0 + kBrick, dy) - 1;
+    const int z0 = bz * kBrick, z1 = min(z0 + kBrick, dz) - 1;
+    const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+    const int total = nx * ny * nz;
+    uint32_t m0 = 0, m1 = 0, m2 = 0;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        int x = x0 + i % nx;
+        int y = y0 + (i / nx) % ny;
+        int z = z0 + i / (nx * ny);
+        int l = lab[((size_t)z * dy + y) * dx + x];
+        if (l > 64) l = 64;   // labels above MAXOBJECTCOUNT never occur via the API
+        if (l < 32) m0 |= 1u << l;
+        else if (l < 64) m1 |= 1u << (l - 32);
+        else m2 |= 1u;
+    }
+    m0 = __reduce_or_sync(0xffffffffu, m0);
+    m1 = __reduce_or_sync(0xffffffffu, m1);
+    m2 = __reduce_or_sync(0xffffffffu, m2);
+    __shared__ uint32_t s[3];
+    if (threadIdx.x < 3) s[threadIdx.x] = 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        atomicOr(&s[0], m0);
+        atomicOr(&s[1], m1);
+        atomicOr(&s[2], m2);
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) out[3 * (size_t)b + threadIdx.x] = s[threadIdx.x];
+}
+
+__global__ void k_fill_labels_zero(uint32_t *out, int nbricks) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < nbricks) {
+        out[3 * (size_t)b + 0] = 1u;   // label 0 only
+        out[3 * (size_t)b + 1] = 0u;
+        out[3 * (size_t)b + 2] = 0u;
+    }
+}
+
+struct VisLabel {
+    const float *lut_alpha;   // nullptr = no table
+    int n;
+    float alpha, ww, wl;
+};
+
+struct VisParams {
+    VisLabel lab[MK_MAX_LABELS];
+};
+
+// One thread per brick.  VR: the brick is visible when, for some label it
+// owns, the LUT alpha over the window of the brick's value range (widened by
+// one LUT entry each side for the linear filter) exceeds kEmptyAlpha.  MIP:
+// the largest windowed value (core/kernel.cu:339-345) over labels with
+// alpha > 0.
+__global__ void __launch_bounds__(256) k_brick_visibility(const short2 *__restrict__ minmax,
+                                                          const uint32_t *__restrict__ labels,
+                                                          int nbricks, VisParams P,
+                                                          uint32_t *vis_bits, float *mip_tmax) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    bool vis = false;
+    float tmax = -INFINITY;
+    if (b < nbricks) {
+        const short2 mm = minmax[b];
+        // Normalized-float read of int16 is v/32767; the kernels scale it by
+        // 32768 (core/kernel.cu:223).  Widen for the filter's rounding.
+        const float k = 32768.0f / 32767.0f;
+        const float hu_lo = (float)mm.x * k - (0.01f + 1e-5f * fabsf((float)mm.x));
+        const float hu_hi = (float)mm.y * k + (0.01f + 1e-5f * fabsf((float)mm.y));
+        for (int w = 0; w < 3; ++w) {
+            uint32_t m = labels[3 * (size_t)b + w];
+            while (m) {
+                const int bit = __ffs(m) - 1;
+                m &= m - 1;
+                const int l = w * 32 + bit;
+                if (l >= MK_MAX_LABELS) break;
+                const VisLabel L = P.lab[l];
+                const float t_lo = (hu_lo - L.wl) / L.ww + 0.5f;
+                const float t_hi = (hu_hi - L.wl) / L.ww + 0.5f;
+                if (L.alpha > 0.0f) tmax = fmaxf(tmax, t_hi);
+                if (L.lut_alpha != nullptr && L.n > 0 && !vis) {
+                    const float tl = fminf(t_lo, 1.0f), th = fminf(t_hi, 1.0f);
+                    int i0 = (int)floorf(tl * L.n - 0.5f) - 1;
+                    int i1 = (int)floorf(th * L.n - 0.5f) + 2;
+                    if (!(tl == tl) || !(th == th)) {
+                        i0 = 0;
+                        i1 = L.n - 1;
+                    }
+                    i0 = max(0, min(i0, L.n - 1));
+                    i1 = max(0, min(i1, L.n - 1));
+                    for (int i = i0; i <= i1; ++i) {
+                        if (L.lut_alpha[i] > kEmptyAlpha) {
+                            vis = true;
+                            break;
+                        }
+                    }
+                }
+            }
+        }
+        if (!(tmax == tmax)) tmax = INFINITY;
+        mip_tmax[b] = tmax;
+    }
+    const uint32_t word = __ballot_sync(0xffffffffu, vis);
+    if ((threadIdx.x & 31) == 0 && b < nbricks + 31) vis_bits[b >> 5] = word;
+}
+
+int upload_linear(const void *host, size_t bytes, void **dptr, cudaStream_t s) {
+    MK_CUDA_TRY(cudaMalloc(dptr, bytes));
+    cudaError_t e = cudaMemcpyAsync(*dptr, host, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaFree(*dptr);
+        *dptr = nullptr;
+        set_last_error(std::string("upload: ") + cudaGetErrorString(e));
+        return MK_ERR_CUDA;
+    }
+    return MK_OK;
+}
+
+int copy_to_array3d(const void *dsrc, size_t elem, int dx, int dy, int dz, cudaArray_t arr,
+                     cudaStream_t s) {
+    cudaMemcpy3DParms p;
+    memset(&p, 0, sizeof(p));
+    p.srcPtr = make_cudaPitchedPtr(const_cast<void *>(dsrc), dx * elem, dx, dy);
+    p.dstArray = arr;
+    p.extent = make_cudaExtent(dx, dy, dz);
+    p.kind = cudaMemcpyDeviceToDevice;
+    MK_CUDA_TRY(cudaMemcpy3DAsync(&p, s));
+    return MK_OK;
+}
+
+void free_tf(VolumeState &v, int l) {
+    if (v.tf_tex[l]) cudaDestroyTextureObject(v.tf_tex[l]);
+    if (v.tf_array[l]) cudaFreeArray(v.tf_array[l]);
+    if (v.d_tf_alpha[l]) cudaFree(v.d_tf_alpha[l]);
+    if (v.tf_len[l] > 0) v.device_bytes -= (size_t)v.tf_len[l] * 20;
+    v.tf_tex[l] = 0;
+    v.tf_array[l] = nullptr;
+    v.d_tf_alpha[l] = nullptr;
+    v.tf_len[l] = 0;
+}
+
+void free_mask(VolumeState &v) {
+    if (v.tex_mask) cudaDestroyTextureObject(v.tex_mask);
+    if (v.mask_array) {
+        cudaFreeArray(v.mask_array);
+        v.device_bytes -= (size_t)v.dims[0] * v.dims[1] * v.dims[2];
+    }
+    v.tex_mask = 0;
+    v.mask_array = nullptr;
+}
+
+}  // namespace
+
+float float_bound_above(double c) {
+    float f = (float)c;
+    if ((double)f <= c) f = nextafterf(f, INFINITY);
+    return f;
+}
+
+BrickView brick_view(const VolumeState *v) {
+    BrickView b;
+    b.visible_bits = v->d_visible;
+    b.mip_tmax = v->d_mip_tmax;
+    b.minmax = v->d_minmax;
+    b.nbx = v->nb[0];
+    b.nby = v->nb[1];
+    b.nbz = v->nb[2];
+    return b;
+}
+
+LabelTable label_table(const VolumeState *v) {
+    LabelTable t;
+    for (int l = 0; l < MK_MAX_LABELS; ++l) {
+        t.tf[l] = v->tf_tex[l];
+        t.alpha[l] = v->params[l][0];
+        t.ww[l] = v->params[l][1];
+        t.wl[l] = v->params[l][2];
+    }
+    return t;
+}
+
+int ensure_device_buffer(VolumeState *v, size_t bytes) {
+    if (v->d_out_bytes >= bytes) return MK_OK;
+    if (v->d_out) {
+        cudaFree(v->d_out);
+        v->device_bytes -= v->d_out_bytes;
+        v->d_out = nullptr;
+        v->d_out_bytes = 0;
+    }
+    MK_CUDA_TRY(cudaMalloc(&v->d_out, bytes));
+    v->d_out_bytes = bytes;
+    v->device_bytes += bytes;
+    return MK_OK;
+}
+
+int ensure_pinned_buffer(VolumeState *v, size_t bytes) {
+    if (v->h_pinned_bytes >= bytes) return MK_OK;
+    if (v->h_pinned) {
+        cudaFreeHost(v->h_pinned);
+        v->h_pinned = nullptr;
+        v->h_pinned_bytes = 0;
+    }
+    MK_CUDA_TRY(cudaMallocHost(&v->h_pinned, bytes));
+    v->h_pinned_bytes = bytes;
+    return MK_OK;
+}
+
+// Copy a finished device output to the caller.  Pinned (or registered)
+// destinations receive the copy directly; pageable ones go through the
+// volume's pinned staging buffer.
+int finish_output(VolumeState *v, void *out, size_t bytes, int out_on_device, cudaStream_t s) {
+    if (out_on_device) return MK_OK;
+    cudaPointerAttributes attr;
+    bool pinned = false;
+    if (cudaPointerGetAttributes(&attr, out) == cudaSuccess)
+        pinned = (attr.type == cudaMemoryTypeHost);
+    else
+        cudaGetLastError();
+    if (pinned) {
+        MK_CUDA_TRY(cudaMemcpyAsync(out, v->d_out, bytes, cudaMemcpyDeviceToHost, s));
+        MK_CUDA_TRY(cudaStreamSynchronize(s));
+        return MK_OK;
+    }
+    int st = ensure_pinned_buffer(v, bytes);
+    if (st != MK_OK) return st;
+    MK_CUDA_TRY(cudaMemcpyAsync(v->h_pinned, v->d_out, bytes, cudaMemcpyDeviceToHost, s));
+    MK_CUDA_TRY(cudaStreamSynchronize(s));
+    memcpy(out, v->h_pinned, bytes);
+    return MK_OK;
+}
+
+int rebuild_brick_maps(VolumeState *v, cudaStream_t s) {
+    if (!v->maps_dirty) return MK_OK;
+    const int nbricks = v->nb[0] * v->nb[1] * v->nb[2];
+    VisParams P;
+    for (int l = 0; l < MK_MAX_LABELS; ++l) {
+        P.lab[l].lut_alpha = v->d_tf_alpha[l];
+        P.lab[l].n = v->tf_len[l];
+        P.lab[l].alpha = v->params[l][0];
+        P.lab[l].ww = v->params[l][1];
+        P.lab[l].wl = v->params[l][2];
+    }
+    const int threads = 256;
+    const int blocks = (nbricks + threads - 1) / threads;
+    k_brick_visibility<<<blocks, threads, 0, s>>>(v->d_minmax, v->d_labels, nbricks, P,
+                                                  v->d_visible, v->d_mip_tmax);
+    MK_CUDA_TRY(cudaGetLastError());
+    v->maps_dirty = false;
+    return MK_OK;
+}
+
+}  // namespace mk
+
+using namespace mk;
+
+extern "C" int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x, int dim_y,
+                                int dim_z, int device) {
+    if (!out || !voxels || dim_x <= 0 || dim_y <= 0 || dim_z <= 0) {
+        set_last_error("mk_volume_create: null pointer or non-positive dimension");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_last_error("mk_volume_create: no CUDA device");
+        return MK_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) {
+        set_last_error("mk_volume_create: device index out of range");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    DeviceGuard guard(device);
+    mk_volume v = new mk_volume_s();
+    VolumeState &st = v->st;
+    st.device = device;
+    st.dims[0] = dim_x;
+    st.dims[1] = dim_y;
+    st.dims[2] = dim_z;
+    for (int l = 0; l < MK_MAX_LABELS; ++l) {
+        st.params[l][0] = 0.0f;   // AlphaAndWWWL() defaults (core/Defines.h:128-132), ww kept positive
+        st.params[l][1] = 1.0f;
+        st.params[l][2] = 0.0f;
+    }
+    int rc = MK_OK;
+    void *d_lin = nullptr;
+    const size_t nvox = (size_t)dim_x * dim_y * dim_z;
+    do {
+        if (cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking) != cudaSuccess) {
+            set_last_error("mk_volume_create: stream creation failed");
+            rc = MK_ERR_CUDA;
+            break;
+        }
+        rc = upload_linear(voxels, nvox * sizeof(short), &d_lin, st.stream);
+        if (rc != MK_OK) break;
+
+        cudaChannelFormatDesc cd = cudaCreateChannelDesc<short>();
+        cudaError_t e = cudaMalloc3DArray(&st.vol_array, &cd, make_cudaExtent(dim_x, dim_y, dim_z));
+        if (e != cudaSuccess) {
+            set_last_error(std::string("cudaMalloc3DArray(volume): ") + cudaGetErrorString(e));
+            rc = (e == cudaErrorMemoryAllocation) ? MK_ERR_OUT_OF_MEMORY : MK_ERR_CUDA;
+            break;
+        }
+        st.device_bytes += nvox * sizeof(short);
+        rc = copy_to_array3d(d_lin, sizeof(short), dim_x, dim_y, dim_z, st.vol_array, st.stream);
+        if (rc != MK_OK) break;
+
+        cudaResourceDesc rd;
+        memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = st.vol_array;
+        cudaTextureDesc td;
+        memset(&td, 0, sizeof(td));
+        td.normalizedCoords = 1;
+        td.filterMode = cudaFilterModeLinear;
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.readMode = cudaReadModeNormalizedFloat;
+        if (cudaCreateTextureObject(&st.tex_linear, &rd, &td, nullptr) != cudaSuccess) {
+            set_last_error("mk_volume_create: linear texture creation failed");
+            rc = MK_ERR_CUDA;
+            break;
+        }
+        td.filterMode = cudaFilterModePoint;
+        if (cudaCreateTextureObject(&st.tex_point, &rd, &td, nullptr) != cudaSuccess) {
+            set_last_error("mk_volume_create: point texture creation failed");
+            rc = MK_ERR_CUDA;
+            break;
+        }
+
+        // brick maps
+        st.nb[0] = (dim_x + kBrick - 1) / kBrick;
+        st.nb[1] = (dim_y + kBrick - 1) / kBrick;
+        st.nb[2] = (dim_z + kBrick - 1) / kBrick;
+        const size_t nbricks = (size_t)st.nb[0] * st.nb[1] * st.nb[2];
+        const size_t nwords = (nbricks + 31) / 32 + 1;
+        if (cudaMalloc(&st.d_minmax, nbricks * sizeof(short2)) != cudaSuccess ||
+            cudaMalloc(&st.d_labels, nbricks * 3 * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&st.d_visible, nwords * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMalloc(&st.d_mip_tmax, nbricks * sizeof(float)) != cudaSuccess ||
+            cudaMalloc(&st.d_counter, sizeof(unsigned long long)) != cudaSuccess) {
+            cudaGetLastError();
+            set_last_error("mk_volume_create: brick map allocation failed");
+            rc = MK_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        st.device_bytes += nbricks * (sizeof(short2) + 3 * sizeof(uint32_t) + sizeof(float)) +
+                           nwords * sizeof(uint32_t) + sizeof(unsigned long long);
+        cudaMemsetAsync(st.d_visible, 0, nwords * sizeof(uint32_t), st.stream);
+        k_brick_minmax<<<(unsigned)nbricks, 256, 0, st.stream>>>((const short *)d_lin, dim_x, dim_y,
+                                                                 dim_z, st.nb[0], st.nb[1],
+                                                                 st.d_minmax);
+        k_fill_labels_zero<<<(unsigned)((nbricks + 255) / 256), 256, 0, st.stream>>>(
+            st.d_labels, (int)nbricks);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            set_last_error(std::string("brick map kernels: ") + cudaGetErrorString(e));
+            rc = MK_ERR_CUDA;
+            break;
+        }
+
+        // ray schedule table: a_{k+1} = fl(a_k + 1/dim_z) (core/kernel.cu:169, 213)
+        const float step = 1.0f / (float)dim_z;
+        const float limit = float_bound_above(1.732);
+        std::vector<float> accu;
+        accu.reserve((size_t)(1.74 * dim_z) + 8);
+        float a = 0.0f;
+        accu.push_back(a);
+        while (a < limit) {
+            a = a + step;
+            accu.push_back(a);
+        }
+        st.accu_len = (int)accu.size();
+        if (cudaMalloc(&st.d_accu, accu.size() * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            set_last_error("mk_volume_create: schedule table allocation failed");
+            rc = MK_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        st.device_bytes += accu.size() * sizeof(float);
+        e = cudaMemcpyAsync(st.d_accu, accu.data(), accu.size() * sizeof(float),
+                            cudaMemcpyHostToDevice, st.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st.stream);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("mk_volume_create: ") + cudaGetErrorString(e));
+            rc = MK_ERR_CUDA;
+            break;
+        }
+    } while (0);
+    if (d_lin) cudaFree(d_lin);
+    if (rc != MK_OK) {
+        mk_volume_destroy(v);
+        return rc;
+    }
+    st.maps_dirty = true;
+    *out = v;
+    return MK_OK;
+}
+
+extern "C" int mk_volume_destroy(mk_volume v) {
+    if (!v) return MK_ERR_INVALID_ARGUMENT;
+    VolumeState &st = v->st;
+    DeviceGuard guard(st.device);
+    if (st.stream) cudaStreamSynchronize(st.stream);
+    for (int l = 0; l < MK_MAX_LABELS; ++l) free_tf(st, l);
+    free_mask(st);
+    if (st.tex_linear) cudaDestroyTextureObject(st.tex_linear);
+    if (st.tex_point) cudaDestroyTextureObject(st.tex_point);
+    if (st.vol_array) cudaFreeArray(st.vol_array);
+    cudaFree(st.d_minmax);
+    cudaFree(st.d_labels);
+    cudaFree(st.d_visible);
+    cudaFree(st.d_mip_tmax);
+    cudaFree(st.d_accu);
+    cudaFree(st.d_out);
+    cudaFree(st.d_counter);
+    if (st.h_pinned) cudaFreeHost(st.h_pinned);
+    if (st.stream) cudaStreamDestroy(st.stream);
+    cudaGetLastError();
+    delete v;
+    return MK_OK;
+}
+
+extern "C" int mk_volume_device_bytes(mk_volume v, size_t *bytes) {
+    if (!v || !bytes) return MK_ERR_INVALID_ARGUMENT;
+    *bytes = v->st.device_bytes;
+    return MK_OK;
+}
+
+extern "C" int mk_volume_dims(mk_volume v, int *dx, int *dy, int *dz) {
+    if (!v || !dx || !dy || !dz) return MK_ERR_INVALID_ARGUMENT;
+    *dx = v->st.dims[0];
+    *dy = v->st.dims[1];
+    *dz = v->st.dims[2];
+    return MK_OK;
+}
+
+extern "C" int mk_volume_set_mask(mk_volume v, const uint8_t *labels) {
+    if (!v) return MK_ERR_INVALID_ARGUMENT;
+    VolumeState &st = v->st;
+    DeviceGuard guard(st.device);
+    const int dx = st.dims[0], dy = st.dims[1], dz = st.dims[2];
+    const size_t nvox = (size_t)dx * dy * dz;
+    const size_t nbricks = (size_t)st.nb[0] * st.nb[1] * st.nb[2];
+    MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    free_mask(st);
+    st.maps_dirty = true;
+    if (!labels) {
+        st.present_labels[0] = 1;
+        st.present_labels[1] = 0;
+        k_fill_labels_zero<<<(unsigned)((nbricks + 255) / 256), 256, 0, st.stream>>>(st.d_labels,
+                                                                                  (int)nbricks);
+        MK_CUDA_TRY(cudaGetLastError());
+        MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
+        return MK_OK;
+    }
+    void *d_lin = nullptr;
+    int rc = upload_linear(labels, nvox, &d_lin, st.stream);
+    if (rc != MK_OK) return rc;
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<unsigned char>();
+    cudaError_t e = cudaMalloc3DArray(&st.mask_array, &cd, make_cudaExtent(dx, dy, dz));
+    if (e != cudaSuccess) {
+        cudaFree(d_lin);
+        set_last_error(std::string("cudaMalloc3DArray(mask): ") + cudaGetErrorString(e));
+        return (e == cudaErrorMemoryAllocation) ? MK_ERR_OUT_OF_MEMORY : MK_ERR_CUDA;
+    }
+    st.device_bytes += nvox;
+    rc = copy_to_array3d(d_lin, 1, dx, dy, dz, st.mask_array, st.stream);
+    if (rc == MK_OK) {
+        cudaResourceDesc rd;
+        memset(&rd, 0, sizeof(rd));
+        rd.resType = cudaResourceTypeArray;
+        rd.res.array.array = st.mask_array;
+        cudaTextureDesc td;
+        memset(&td, 0, sizeof(td));
+        td.normalizedCoords = 0;
+        td.filterMode = cudaFilterModePoint;
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeClamp;
+        td.readMode = cudaReadModeElementType;
+        if (cudaCreateTextureObject(&st.tex_mask, &rd, &td, nullptr) != cudaSuccess) {
+            set_last_error("mk_volume_set_mask: texture creation failed");
+            rc = MK_ERR_CUDA;
+        }
+    }
+    if (rc == MK_OK) {
+        k_brick_labels<<<(unsigned)nbricks, 256, 0, st.stream>>>((const unsigned char *)d_lin, dx,
+                                                                 dy, dz, st.nb[0], st.nb[1],
+                                                                 st.d_labels);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st.stream);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("mk_volume_set_mask: ") + cudaGetErrorString(e));
+            rc = MK_ERR_CUDA;
+        }
+    }
+    cudaFree(d_lin);
+    if (rc != MK_OK) {
+        free_mask(st);
+        return rc;
+    }
+    // labels present anywhere (host-side scan; used to size per-ray state)
+    uint64_t pres[2] = {0, 0};
+    for (size_t i = 0; i < nvox; ++i) {
+        const int l = labels[i] > 64 ? 64 : labels[i];
+        pres[l >> 6] |= 1ull << (l & 63);
+    }
+    st.present_labels[0] = pres[0];
+    st.present_labels[1] = pres[1];
+    return MK_OK;
+}
+
+extern "C" int mk_volume_set_transfer_function(mk_volume v, int label, const float *rgba,
+                                               int n_entries) {
+    if (!v || label < 0 || label >= MK_MAX_LABELS) {
+        set_last_error("mk_volume_set_transfer_function: bad volume or label");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &st = v->st;
+    DeviceGuard guard(st.device);
+    MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    free_tf(st, label);
+    st.maps_dirty = true;
+    if (!rgba || n_entries <= 0) return MK_OK;   // label becomes transparent
+    if (n_entries > 65536) {
+        set_last_error("mk_volume_set_transfer_function: more than 65536 entries");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float4>();
+    MK_CUDA_TRY(cudaMallocArray(&st.tf_array[label], &cd, n_entries, 1));
+    MK_CUDA_TRY(cudaMemcpy2DToArray(st.tf_array[label], 0, 0, rgba, n_entries * sizeof(float4),
+                                    n_entries * sizeof(float4), 1, cudaMemcpyHostToDevice));
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = st.tf_array[label];
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.normalizedCoords = 1;
+    td.filterMode = cudaFilterModeLinear;
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.readMode = cudaReadModeElementType;
+    MK_CUDA_TRY(cudaCreateTextureObject(&st.tf_tex[label], &rd, &td, nullptr));
+    std::vector<float> alpha(n_entries);
+    for (int i = 0; i < n_entries; ++i) alpha[i] = rgba[4 * i + 3];
+    MK_CUDA_TRY(cudaMalloc(&st.d_tf_alpha[label], n_entries * sizeof(float)));
+    MK_CUDA_TRY(cudaMemcpy(st.d_tf_alpha[label], alpha.data(), n_entries * sizeof(float),
+                           cudaMemcpyHostToDevice));
+    st.tf_len[label] = n_entries;
+    st.device_bytes += (size_t)n_entries * 20;
+    return MK_OK;
+}
+
+extern "C" int mk_volume_set_label_params(mk_volume v, const float *alpha_ww_wl, int n_labels) {
+    if (!v || !alpha_ww_wl || n_labels <= 0 || n_labels > MK_MAX_LABELS) {
+        set_last_error("mk_volume_set_label_params: bad arguments");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    for (int l = 0; l < n_labels; ++l) {
+        if (!(alpha_ww_wl[3 * l + 1] > 0.0f)) {
+            set_last_error("mk_volume_set_label_params: window width must be > 0");
+            return MK_ERR_INVALID_ARGUMENT;
+        }
+    }
+    VolumeState &st = v->st;
+    for (int l = 0; l < n_labels; ++l) {
+        st.params[l][0] = alpha_ww_wl[3 * l + 0];
+        st.params[l][1] = alpha_ww_wl[3 * l + 1];
+        st.params[l][2] = alpha_ww_wl[3 * l + 2];
+    }
+    st.maps_dirty = true;
+    return MK_OK;
+}
+
+extern "C" int mk_volume_synchronize(mk_volume v, void *stream) {
+    if (!v) return MK_ERR_INVALID_ARGUMENT;
+    DeviceGuard guard(v->st.device);
+    cudaStream_t s = stream ? (cudaStream_t)stream : v->st.stream;
+    MK_CUDA_TRY(cudaStreamSynchronize(s));
+    return MK_OK;
+}

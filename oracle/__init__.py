@@ -1,0 +1,200 @@
+"""TEST INFRASTRUCTURE -- the parity oracle for MonkeyGL's ray-casting path.
+
+Only tests/, __graft_entry__.smoke() and bench.py (CPU baseline and reference
+arm) import this package.  The product library never does.
+
+* ``cpu``      -- ctypes wrapper of lib/libmkoracle.so, the C restatement in
+                  mk_oracle.c (texture-emulating FP32 and exact FP64 modes).
+* ``RefGPU``   -- MonkeyGL's own CUDA kernels (_ref/libmkref_gpu.so, built from
+                  the unmodified core/kernel.cu and core/CuDataManager.cu).
+* ``RefHost``  -- MonkeyGL's own host library with kernel-argument capture
+                  (_ref/libmkref_host.so), used to generate golden vectors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+CPU_LIB = HERE / "lib" / "libmkoracle.so"
+REF_GPU_LIB = HERE / "_ref" / "libmkref_gpu.so"
+REF_HOST_LIB = HERE / "_ref" / "libmkref_host.so"
+LABELS = 65
+VR_FLOATS = 32 + 3 * LABELS
+
+TEX32, EXACT64 = 0, 1
+
+
+def _vp(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class _MkoVolume(C.Structure):
+    _fields_ = [("vox", C.c_void_p), ("dim", C.c_int * 3), ("mask", C.c_void_p),
+                ("lut", C.c_void_p * LABELS), ("lut_len", C.c_int * LABELS)]
+
+
+_cpu = None
+
+
+def cpu():
+    global _cpu
+    if _cpu is None:
+        if not CPU_LIB.exists():
+            raise FileNotFoundError(f"{CPU_LIB} missing; run `make -C oracle oracle`")
+        L = C.CDLL(str(CPU_LIB))
+        L.mko_render_vr.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                    C.c_int, C.c_void_p, C.POINTER(C.c_uint64)]
+        L.mko_render_plane.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, C.c_void_p]
+        L.mko_render_cpr.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_int, C.c_void_p]
+        L.mko_tex3d_linear.argtypes = [C.POINTER(_MkoVolume), C.c_float, C.c_float, C.c_float]
+        L.mko_tex3d_linear.restype = C.c_float
+        L.mko_tex3d_point.argtypes = [C.POINTER(_MkoVolume), C.c_float, C.c_float, C.c_float]
+        L.mko_tex3d_point.restype = C.c_float
+        L.mko_tex1d_lut.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_void_p]
+        L.mko_set_weight_mode.argtypes = [C.c_int]
+        _cpu = L
+    return _cpu
+
+
+class CpuVolume:
+    """A volume for the CPU oracle (keeps its numpy buffers alive)."""
+
+    def __init__(self, voxels, labels=None):
+        self.vox = np.ascontiguousarray(voxels, dtype=np.int16)
+        self.mask = None if labels is None else np.ascontiguousarray(labels, dtype=np.uint8)
+        self.luts = [None] * LABELS
+        self.s = _MkoVolume()
+        self.s.vox = self.vox.ctypes.data
+        dz, dy, dx = self.vox.shape
+        self.s.dim[0], self.s.dim[1], self.s.dim[2] = dx, dy, dz
+        self.s.mask = self.mask.ctypes.data if self.mask is not None else None
+
+    def set_lut(self, label, lut):
+        if lut is None:
+            self.luts[label] = None
+            self.s.lut[label] = None
+            self.s.lut_len[label] = 0
+            return
+        t = np.ascontiguousarray(lut, dtype=np.float32).reshape(-1, 4)
+        self.luts[label] = t
+        self.s.lut[label] = t.ctypes.data
+        self.s.lut_len[label] = t.shape[0]
+
+    def render_vr(self, w, h, rtype, flat_params, precision=TEX32, threads=0, with_samples=False):
+        out = np.zeros((h, w, 3), np.uint8)
+        n = C.c_uint64(0)
+        p = np.ascontiguousarray(flat_params, dtype=np.float32)
+        rc = cpu().mko_render_vr(C.byref(self.s), w, h, rtype, _vp(p), precision, threads, _vp(out), C.byref(n))
+        if rc:
+            raise RuntimeError(f"mko_render_vr failed: {rc}")
+        return (out, n.value) if with_samples else out
+
+    def render_plane(self, w, h, flat_params, mpr_type, nearest, precision=TEX32, threads=0):
+        out = np.zeros((h, w), np.int16)
+        p = np.ascontiguousarray(flat_params, dtype=np.float32)
+        rc = cpu().mko_render_plane(C.byref(self.s), w, h, _vp(p), mpr_type, int(nearest), precision, threads,
+                                    _vp(out))
+        if rc:
+            raise RuntimeError(f"mko_render_plane failed: {rc}")
+        return out
+
+    def render_cpr(self, w, pts, dirs, invert_z, precision=TEX32, threads=0):
+        pts = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        dirs = np.ascontiguousarray(dirs, np.float64).reshape(-1, 3)
+        h = pts.shape[0]
+        out = np.zeros((h, w), np.int16)
+        rc = cpu().mko_render_cpr(C.byref(self.s), w, h, _vp(pts), _vp(dirs), int(bool(invert_z)), precision,
+                                  threads, _vp(out))
+        if rc:
+            raise RuntimeError(f"mko_render_cpr failed: {rc}")
+        return out
+
+    def tex3d_linear(self, x, y, z):
+        return cpu().mko_tex3d_linear(C.byref(self.s), x, y, z)
+
+    def tex3d_point(self, x, y, z):
+        return cpu().mko_tex3d_point(C.byref(self.s), x, y, z)
+
+
+def set_weight_mode(mode: int):
+    cpu().mko_set_weight_mode(mode)
+
+
+def ref_gpu_available() -> bool:
+    return REF_GPU_LIB.exists()
+
+
+class RefGPU:
+    """MonkeyGL's own CUDA path (one global volume, as in MonkeyGL)."""
+
+    _L = None
+
+    def __init__(self):
+        if RefGPU._L is None:
+            if not REF_GPU_LIB.exists():
+                raise FileNotFoundError(f"{REF_GPU_LIB} missing; run `make -C oracle ref-gpu`")
+            L = C.CDLL(str(REF_GPU_LIB))
+            L.mkref_volume.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+            L.mkref_mask.argtypes = [C.c_void_p]
+            L.mkref_tf.argtypes = [C.c_int, C.c_void_p, C.c_int]
+            L.mkref_render.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
+            L.mkref_render_kernel_ms.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
+            L.mkref_render_kernel_ms.restype = C.c_double
+            L.mkref_plane.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
+            L.mkref_cpr.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+            RefGPU._L = L
+        self.L = RefGPU._L
+
+    def device_count(self):
+        return self.L.mkref_device_count()
+
+    def set_volume(self, vox):
+        self.vox = np.ascontiguousarray(vox, dtype=np.int16)
+        dz, dy, dx = self.vox.shape
+        assert self.L.mkref_volume(_vp(self.vox), dx, dy, dz) == 0
+
+    def set_mask(self, labels):
+        if labels is None:
+            assert self.L.mkref_mask(None) == 0
+        else:
+            m = np.ascontiguousarray(labels, dtype=np.uint8)
+            assert self.L.mkref_mask(_vp(m)) == 0
+
+    def clear_tfs(self):
+        self.L.mkref_clear_tfs()
+
+    def set_lut(self, label, lut):
+        t = np.ascontiguousarray(lut, dtype=np.float32).reshape(-1, 4)
+        assert self.L.mkref_tf(label, _vp(t), t.shape[0]) == 0
+
+    def render(self, w, h, rtype, flat_params):
+        out = np.zeros((h, w, 3), np.uint8)
+        p = np.ascontiguousarray(flat_params, dtype=np.float32)
+        assert self.L.mkref_render(_vp(out), w, h, _vp(p), rtype) == 0
+        return out
+
+    def render_into(self, out, w, h, rtype, p):
+        return self.L.mkref_render(_vp(out), w, h, _vp(p), rtype)
+
+    def kernel_ms(self, w, h, rtype, flat_params, reps=5):
+        p = np.ascontiguousarray(flat_params, dtype=np.float32)
+        return self.L.mkref_render_kernel_ms(w, h, _vp(p), rtype, reps)
+
+    def plane(self, w, h, flat_params, mpr_type, nearest):
+        out = np.zeros((h, w), np.int16)
+        p = np.ascontiguousarray(flat_params, dtype=np.float32)
+        assert self.L.mkref_plane(_vp(out), w, h, _vp(p), mpr_type, int(nearest)) == 0
+        return out
+
+    def cpr(self, w, pts, dirs, invert_z):
+        pts = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        dirs = np.ascontiguousarray(dirs, np.float64).reshape(-1, 3)
+        h = pts.shape[0]
+        out = np.zeros((h, w), np.int16)
+        assert self.L.mkref_cpr(_vp(out), w, h, _vp(pts), _vp(dirs), int(bool(invert_z))) == 0
+        return out
