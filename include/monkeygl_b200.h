@@ -198,6 +198,17 @@ int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out,
 int mk_count_vr_samples(mk_volume vol, const mk_vr_params *params, uint64_t *samples);
 
 /*
+ * Measurement pass over the same schedule as mk_count_vr_samples: besides the
+ * sample count, the number of distinct int16 voxels inside the trilinear
+ * footprints of every fetch (value and gradient taps) and of distinct label
+ * voxels read.  These give the algorithmic bytes of a frame
+ * (2 * voxels + label_voxels + output bytes).  Allocates two temporary bitsets
+ * of one bit per voxel; does not render.
+ */
+int mk_count_vr_footprint(mk_volume vol, const mk_vr_params *params, uint64_t *samples,
+                          uint64_t *voxels, uint64_t *label_voxels);
+
+/*
  * Reslice a plane (MPR) into width*height int16 values.  Replaces
  * cu_renderPlane_{Average,MIP,MinIP} (core/kernel.cu:570-837).
  */

@@ -16,6 +16,14 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libmonkeygl_b200.so"
 MAX_LABELS = 65
 
 MK_OK = 0
+MK_ERR_INVALID_ARGUMENT = 1
+MK_ERR_CUDA = 2
+MK_ERR_OUT_OF_MEMORY = 3
+MK_ERR_NOT_READY = 4
+MK_ERR_BUDGET = 5
+MK_ERR_TIMEOUT = 6
+MK_ERR_NO_DEVICE = 7
+MK_ERR_QUEUE_FULL = 8
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not ready",
     5: "device memory budget exceeded", 6: "timed out", 7: "no CUDA device", 8: "queue full",
@@ -73,6 +81,8 @@ _SIGS = {
     "mk_volume_set_label_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "mk_render_vr": (C.c_int, [C.c_void_p, C.POINTER(VRParams), C.c_void_p, C.c_int, C.c_void_p]),
     "mk_count_vr_samples": (C.c_int, [C.c_void_p, C.POINTER(VRParams), C.POINTER(C.c_uint64)]),
+    "mk_count_vr_footprint": (C.c_int, [C.c_void_p, C.POINTER(VRParams), C.POINTER(C.c_uint64),
+                                        C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "mk_render_plane": (C.c_int, [C.c_void_p, C.POINTER(PlaneParams), C.c_void_p, C.c_int, C.c_void_p]),
     "mk_render_plane_u8": (C.c_int, [C.c_void_p, C.POINTER(PlaneParams), C.c_float, C.c_float,
                                      C.c_void_p, C.c_int, C.c_void_p]),
@@ -194,6 +204,13 @@ class Volume:
         n = C.c_uint64(0)
         _check(lib().mk_count_vr_samples(self.handle, C.byref(params), C.byref(n)), "mk_count_vr_samples")
         return n.value
+
+    def count_footprint(self, params: VRParams):
+        """(samples, distinct voxels, distinct label voxels) of the reference schedule."""
+        a, b, c = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        _check(lib().mk_count_vr_footprint(self.handle, C.byref(params), C.byref(a), C.byref(b), C.byref(c)),
+               "mk_count_vr_footprint")
+        return a.value, b.value, c.value
 
     def render_plane(self, params: PlaneParams, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:

@@ -64,6 +64,8 @@ struct RayParams {
     int skip;
     uint8_t *out;
     unsigned long long *counter; // sample counting mode
+    uint32_t *vox_bits;          // counting mode: voxels inside trilinear footprints (may be null)
+    uint32_t *lab_bits;          // counting mode: label voxels read (may be null)
 };
 
 struct LabelSmem {
@@ -171,6 +173,45 @@ __device__ __forceinline__ int steps_in_brick(const float3 &pv, const float3 &dv
         else if (dd[k] < -1e-6f) t = fminf(t, (pp[k] - lo[k] - e) / -dd[k]);
     }
     return t > 0.0f ? (int)t : 0;
+}
+
+// Counting mode: mark the eight texels of a trilinear fetch at normalized
+// position (x, y, z) under clamp addressing.
+__device__ void mark_footprint(const RayParams &P, float x, float y, float z) {
+    if (!P.vox_bits) return;
+    int lo[3], hi[3];
+    const float c[3] = {x, y, z};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int i0 = (int)floorf(c[k] * P.fdim[k] - 0.5f);
+        lo[k] = min(max(i0, 0), P.dimi[k] - 1);
+        hi[k] = min(max(i0 + 1, 0), P.dimi[k] - 1);
+    }
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                const size_t idx = ((size_t)(dz ? hi[2] : lo[2]) * P.dimi[1] + (dy ? hi[1] : lo[1])) *
+                                       P.dimi[0] + (dx ? hi[0] : lo[0]);
+                atomicOr(&P.vox_bits[idx >> 5], 1u << (idx & 31));
+            }
+}
+
+__device__ void mark_gradient(const RayParams &P, float3 pos) {
+    mark_footprint(P, pos.x + P.sv[0], pos.y, pos.z);
+    mark_footprint(P, pos.x - P.sv[0], pos.y, pos.z);
+    mark_footprint(P, pos.x, pos.y + P.sv[1], pos.z);
+    mark_footprint(P, pos.x, pos.y - P.sv[1], pos.z);
+    mark_footprint(P, pos.x, pos.y, pos.z + P.sv[2]);
+    mark_footprint(P, pos.x, pos.y, pos.z - P.sv[2]);
+}
+
+__device__ void mark_label(const RayParams &P, int ix, int iy, int iz) {
+    if (!P.lab_bits) return;
+    ix = min(max(ix, 0), P.dimi[0] - 1);
+    iy = min(max(iy, 0), P.dimi[1] - 1);
+    iz = min(max(iz, 0), P.dimi[2] - 1);
+    const size_t idx = ((size_t)iz * P.dimi[1] + iy) * P.dimi[0] + ix;
+    atomicOr(&P.lab_bits[idx >> 5], 1u << (idx & 31));
 }
 
 // Central-difference normal and headlight shading (core/kernel.cu:49-81).
@@ -314,7 +355,11 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
                             continue;
                         }
                     }
-                    if (COUNT) ++nsamples;
+                    if (COUNT) {
+                        ++nsamples;
+                        mark_footprint(P, pos.x, pos.y, pos.z);
+                        if (mask) mark_label(P, ix, iy, iz);
+                    }
                     const int label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
                     float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
                     temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
@@ -354,6 +399,7 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
                             else if (sl == -1) ok = true;
                             else ok = s_acc[sl][tid] < S.alpha[label];
                             if (ok) {
+                                mark_gradient(P, pos);
                                 if (TRACK == kTrackLocal) accLocal[label] += (1.0f - A) * col.w;
                                 else if (TRACK == kTrackShared && sl >= 0) s_acc[sl][tid] += (1.0f - A) * col.w;
                                 A += (1.0f - A) * col.w;
@@ -400,8 +446,12 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
                         }
                     }
                     const int label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
+                    if (COUNT && mask) mark_label(P, ix, iy, iz);
                     if (S.alpha[label] > 0) {
-                        if (COUNT) ++nsamples;
+                        if (COUNT) {
+                            ++nsamples;
+                            mark_footprint(P, pos.x, pos.y, pos.z);
+                        }
                         float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
                         temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
                         if (A < temp) A = temp;
@@ -445,12 +495,16 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
                             continue;
                         }
                     }
-                    if (COUNT) ++nsamples;
+                    if (COUNT) {
+                        ++nsamples;
+                        mark_footprint(P, pos.x, pos.y, pos.z);
+                    }
                     const float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
                     if (temp <= 400) {
                         a += fStep;
                         continue;
                     }
+                    if (COUNT) mark_gradient(P, pos);
                     float3 N;
                     N.x = tex3D<float>(vol, pos.x + P.sv[0], pos.y, pos.z) - tex3D<float>(vol, pos.x - P.sv[0], pos.y, pos.z);
                     N.y = tex3D<float>(vol, pos.x, pos.y + P.sv[1], pos.z) - tex3D<float>(vol, pos.x, pos.y - P.sv[1], pos.z);
@@ -593,6 +647,8 @@ static int fill_params(const VolumeState &v, const mk_vr_params *p, RayParams &P
     P.skip = (p->flags & MK_VR_NO_SKIP) ? 0 : 1;
     P.out = nullptr;
     P.counter = nullptr;
+    P.vox_bits = nullptr;
+    P.lab_bits = nullptr;
     return MK_OK;
 }
 
@@ -628,6 +684,14 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     return finish_output(&v, out, bytes, out_on_device, s);
 }
 
+__global__ void k_popcount(const uint32_t *__restrict__ bits, size_t nwords, unsigned long long *out) {
+    unsigned long long c = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nwords; i += (size_t)gridDim.x * blockDim.x)
+        c += __popc(bits[i]);
+    c = __reduce_add_sync(0xffffffffu, (unsigned)c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
 extern "C" int mk_count_vr_samples(mk_volume vol, const mk_vr_params *params, uint64_t *samples) {
     if (!vol || !samples) {
         set_last_error("mk_count_vr_samples: null argument");
@@ -652,4 +716,56 @@ extern "C" int mk_count_vr_samples(mk_volume vol, const mk_vr_params *params, ui
     MK_CUDA_TRY(cudaStreamSynchronize(s));
     *samples = h;
     return MK_OK;
+}
+
+extern "C" int mk_count_vr_footprint(mk_volume vol, const mk_vr_params *params, uint64_t *samples,
+                                     uint64_t *voxels, uint64_t *label_voxels) {
+    if (!vol || !samples || !voxels || !label_voxels) {
+        set_last_error("mk_count_vr_footprint: null argument");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &v = vol->st;
+    RayParams P;
+    int rc = fill_params(v, params, P);
+    if (rc != MK_OK) return rc;
+    cudaSetDevice(v.device);
+    cudaStream_t s = v.stream;
+    const size_t nvox = (size_t)v.dims[0] * v.dims[1] * v.dims[2];
+    const size_t nwords = (nvox + 31) / 32;
+    uint32_t *bits = nullptr;
+    unsigned long long *cnt = nullptr;
+    MK_CUDA_TRY(cudaMalloc(&bits, 2 * nwords * sizeof(uint32_t)));
+    if (cudaMalloc(&cnt, 3 * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaFree(bits);
+        set_last_error("mk_count_vr_footprint: allocation failed");
+        return MK_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemsetAsync(bits, 0, 2 * nwords * sizeof(uint32_t), s);
+    cudaMemsetAsync(cnt, 0, 3 * sizeof(unsigned long long), s);
+    P.skip = 0;
+    P.counter = cnt;
+    P.vox_bits = bits;
+    P.lab_bits = bits + nwords;
+    rc = rebuild_brick_maps(&v, s);
+    if (rc == MK_OK) {
+        launch_raycast<true>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
+                             label_table(&v), brick_view(&v), s);
+        k_popcount<<<1184, 256, 0, s>>>(bits, nwords, cnt + 1);
+        k_popcount<<<1184, 256, 0, s>>>(bits + nwords, nwords, cnt + 2);
+        unsigned long long h[3] = {0, 0, 0};
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            set_last_error(std::string("mk_count_vr_footprint: ") + cudaGetErrorString(e));
+            rc = MK_ERR_CUDA;
+        } else {
+            *samples = h[0];
+            *voxels = h[1];
+            *label_voxels = h[2];
+        }
+    }
+    cudaFree(bits);
+    cudaFree(cnt);
+    return rc;
 }

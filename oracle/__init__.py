@@ -47,6 +47,8 @@ def cpu():
         L = C.CDLL(str(CPU_LIB))
         L.mko_render_vr.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                     C.c_int, C.c_void_p, C.POINTER(C.c_uint64)]
+        L.mko_render_vr_rows.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                         C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_uint64)]
         L.mko_render_plane.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
                                        C.c_int, C.c_int, C.c_void_p]
         L.mko_render_cpr.argtypes = [C.POINTER(_MkoVolume), C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
@@ -93,6 +95,16 @@ class CpuVolume:
         if rc:
             raise RuntimeError(f"mko_render_vr failed: {rc}")
         return (out, n.value) if with_samples else out
+
+    def render_vr_rows(self, w, h, rtype, flat_params, row0, row_step, nrows, precision=TEX32, threads=0):
+        out = np.zeros((nrows, w, 3), np.uint8)
+        n = C.c_uint64(0)
+        p = np.ascontiguousarray(flat_params, dtype=np.float32)
+        rc = cpu().mko_render_vr_rows(C.byref(self.s), w, h, rtype, _vp(p), precision, threads, row0, row_step,
+                                      nrows, _vp(out), C.byref(n))
+        if rc:
+            raise RuntimeError(f"mko_render_vr_rows failed: {rc}")
+        return out, n.value
 
     def render_plane(self, w, h, flat_params, mpr_type, nearest, precision=TEX32, threads=0):
         out = np.zeros((h, w), np.int16)

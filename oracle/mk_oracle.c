@@ -494,7 +494,13 @@ static void pixel_d(const mko_volume *v, const vrp *q, int type, int w, int h, i
 
 int mko_render_vr(const mko_volume *v, int w, int h, int type, const float *params, int precision,
                   int nthreads, uint8_t *out_rgb, uint64_t *samples) {
+    return mko_render_vr_rows(v, w, h, type, params, precision, nthreads, 0, 1, h, out_rgb, samples);
+}
+
+int mko_render_vr_rows(const mko_volume *v, int w, int h, int type, const float *params, int precision,
+                       int nthreads, int row0, int row_step, int nrows, uint8_t *out_rgb, uint64_t *samples) {
     if (!v || !v->vox || !params || !out_rgb || w <= 0 || h <= 0 || type < 0 || type > 2) return 1;
+    if (row0 < 0 || row_step <= 0 || nrows <= 0 || row0 + (nrows - 1) * row_step >= h) return 1;
     vrp q;
     unpack_vr(params, &q);
     uint64_t total = 0;
@@ -502,9 +508,10 @@ int mko_render_vr(const mko_volume *v, int w, int h, int type, const float *para
     int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(+ : total)
 #endif
-    for (int y = 0; y < h; ++y) {
+    for (int r = 0; r < nrows; ++r) {
+        const int y = row0 + r * row_step;
         for (int x = 0; x < w; ++x) {
-            uint8_t *o = out_rgb + ((size_t)y * w + x) * 3;
+            uint8_t *o = out_rgb + ((size_t)r * w + x) * 3;
             uint64_t n = 0;
             if (precision == MKO_EXACT64) pixel_d(v, &q, type, w, h, x, y, o);
             else if (type == MKO_VR) vr_pixel_f(v, &q, w, h, x, y, o, &n);

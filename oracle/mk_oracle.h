@@ -61,6 +61,12 @@ void mko_set_weight_mode(int mode);
 int mko_render_vr(const mko_volume *v, int w, int h, int type, const float *params,
                   int precision, int nthreads, uint8_t *out_rgb, uint64_t *samples);
 
+/* The same for the rows row0, row0 + row_step, ... (nrows of them) of a
+ * w*h frame, written consecutively to out_rgb (nrows*w*3 bytes). */
+int mko_render_vr_rows(const mko_volume *v, int w, int h, int type, const float *params,
+                       int precision, int nthreads, int row0, int row_step, int nrows,
+                       uint8_t *out_rgb, uint64_t *samples);
+
 /* d_renderPlane_{Average,MIP,MinIP} (core/kernel.cu:570-793). mpr_type: 0
  * Average, 1 MIP, 2 MinIP; nearest selects point sampling. */
 int mko_render_plane(const mko_volume *v, int w, int h, const float *params, int mpr_type,

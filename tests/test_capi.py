@@ -1,0 +1,81 @@
+"""The C ABI of include/monkeygl_b200.h without a GPU: the library loads,
+exports every declared entry point, validates arguments before touching the
+device and reports a missing device as MK_ERR_NO_DEVICE instead of exiting
+(MonkeyGL's checkCudaErrors exits the process, cuda_common/helper_cuda.h)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from monkeygl_b200 import capi
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "monkeygl_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*|void)\s+\*?\s*(mk_\w+)\s*\(", text, re.M)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ("mk_volume_create", "mk_render_vr", "mk_render_plane", "mk_render_cpr",
+                 "mk_volume_set_mask", "mk_volume_set_transfer_function"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    assert set(declared_functions()) <= set(capi.exported_symbols())
+
+
+def test_status_strings():
+    L = capi.lib()
+    assert L.mk_status_string(0) == b"ok"
+    assert L.mk_status_string(7) == b"no CUDA device"
+    assert L.mk_status_string(999) == b"unknown status"
+    assert L.mk_version().decode().count(".") == 2
+
+
+def test_device_count_never_fails():
+    assert capi.device_count() >= 0
+
+
+def test_create_validates_before_device():
+    L = capi.lib()
+    h = C.c_void_p()
+    vox = np.zeros(8, np.int16)
+    assert L.mk_volume_create(C.byref(h), None, 2, 2, 2, 0) == capi.MK_ERR_INVALID_ARGUMENT
+    assert L.mk_volume_create(C.byref(h), C.c_void_p(vox.ctypes.data), 0, 2, 2, 0) == 1
+    assert L.mk_volume_create(None, C.c_void_p(vox.ctypes.data), 2, 2, 2, 0) == 1
+    assert b"dimension" in L.mk_last_error() or b"null" in L.mk_last_error()
+
+
+def test_entry_points_reject_null_handles():
+    L = capi.lib()
+    p = capi.VRParams()
+    buf = np.zeros(16, np.uint8)
+    assert L.mk_render_vr(None, C.byref(p), C.c_void_p(buf.ctypes.data), 0, None) == 1
+    assert L.mk_render_plane(None, C.byref(capi.PlaneParams()), C.c_void_p(buf.ctypes.data), 0, None) == 1
+    assert L.mk_render_cpr(None, 4, 4, None, None, 0, None, 0, None) == 1
+    assert L.mk_volume_set_mask(None, None) == 1
+    assert L.mk_volume_set_transfer_function(None, 0, None, 0) == 1
+    assert L.mk_volume_set_label_params(None, None, 1) == 1
+    assert L.mk_volume_destroy(None) == 1
+    n = C.c_uint64()
+    assert L.mk_count_vr_samples(None, C.byref(p), C.byref(n)) == 1
+
+
+@pytest.mark.skipif(capi.device_count() > 0, reason="a CUDA device is present")
+def test_no_device_is_a_status_not_an_exit():
+    with pytest.raises(capi.MonkeyGLError) as ei:
+        capi.Volume(np.zeros((4, 4, 4), np.int16))
+    assert ei.value.status == 7
