@@ -76,8 +76,14 @@ struct LabelSmem {
     signed char slot[MK_MAX_LABELS];   // >=0 tracked slot, -1 uncapped, -2 never composites
 };
 
+// The camera-matrix product of core/kernel.cu:31-38 (helper_math dot()).
+// nvcc fuses MonkeyGL's x*x' + y*y' + z*z' left to right into two FMAs; the
+// same expression written plainly here is contracted differently in this
+// kernel, so the order is spelled out.  Comparing images against MonkeyGL's
+// kernel on tilted views, this is the only order of the six fused and one
+// unfused forms that reproduces every sample position.
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
-    return ax * bx + ay * by + az * bz;   // same expression shape as helper_math dot()
+    return __fmaf_rn(az, bz, __fmaf_rn(ay, by, __fmul_rn(ax, bx)));
 }
 
 // One sample position of the reference schedule (core/kernel.cu:197-206).
