@@ -234,6 +234,28 @@ int mk_render_cpr(mk_volume vol, int width, int height, const double *points,
                   const double *dirs, int invert_z, int16_t *out, int out_on_device,
                   void *stream);
 
+/*
+ * mk_render_cpr without any device allocation.  It has no counterpart in
+ * MonkeyGL: it is for callers that cannot call cudaMalloc (a host with a
+ * fixed, pre-planned device-memory budget, a framework whose caching
+ * allocator already holds the memory, a render loop that must not stall on
+ * the synchronisation cudaMalloc/cudaFree can imply).  Same rows, pixels and
+ * fill value as mk_render_cpr; the caller provides the device output buffer
+ * (width*height int16) and the path as host doubles.
+ *   - The per-row table lives in a fixed device array of 4096 rows (192 KiB)
+ *     that every GPU loading this library holds until the process exits;
+ *     height > 4096 is rejected with MK_ERR_INVALID_ARGUMENT and a message.
+ *   - The first call on a device looks up that array's device address; make
+ *     that first call before any stream capture.
+ *   - The call is asynchronous on `stream` (NULL = the volume's stream).
+ *     Every call shares the one array (each call overwrites the rows it
+ *     uses; nothing needs to start at zero), so calls that overlap on the
+ *     GPU, e.g. on two streams, race; calls on one stream are ordered.
+ *   - It calls no cudaMalloc, cudaFree or other allocating routine.
+ */
+int mk_render_cpr_noalloc(mk_volume vol, int width, int height, const double *points,
+                          const double *dirs, int invert_z, int16_t *out_device, void *stream);
+
 /* Wait for all work queued on `stream` (NULL = the volume's stream). */
 int mk_volume_synchronize(mk_volume vol, void *stream);
 

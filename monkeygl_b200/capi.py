@@ -88,6 +88,8 @@ _SIGS = {
                                      C.c_void_p, C.c_int, C.c_void_p]),
     "mk_render_cpr": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                 C.c_void_p, C.c_int, C.c_void_p]),
+    "mk_render_cpr_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.c_void_p, C.c_void_p]),
     "mk_volume_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
 }
 

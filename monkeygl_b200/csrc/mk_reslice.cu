@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "mk_internal.h"
@@ -248,4 +250,79 @@ extern "C" int mk_render_cpr(mk_volume vol, int width, int height, const double 
         return MK_OK;
     }
     return finish_output(&v, out, out_bytes, 0, s);
+}
+
+// ---------------------------------------------------------------------------
+// CPR without allocation.
+//
+// Some callers cannot call cudaMalloc: hosts that hand the GPU a fixed,
+// pre-planned memory budget (certified medical viewers, embedded consoles),
+// frameworks whose own caching allocator has reserved the device memory, and
+// render loops that must not stall on the device-wide synchronisation that
+// cudaMalloc/cudaFree can imply.  mk_render_cpr_noalloc serves them: the
+// caller passes the path (host doubles) and a device output buffer, and the
+// per-row table the kernel reads lives in the fixed array below, which every
+// GPU that loads this library holds until the process exits.
+constexpr int kNoAllocCprRows = 4096;   // 4096 rows x 48 B = 192 KiB
+static __device__ __align__(256) CprRow g_noalloc_cpr_rows[kNoAllocCprRows];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;                         // guards the two tables below
+void *g_noalloc_rows_dev[kNoAllocMaxDevices] = {};  // device address of the array, per device
+CprRow g_noalloc_rows_host[kNoAllocCprRows];        // host staging of one call's rows
+}  // namespace
+
+extern "C" int mk_render_cpr_noalloc(mk_volume vol, int width, int height, const double *points,
+                                     const double *dirs, int invert_z, int16_t *out_device,
+                                     void *stream) {
+    if (!vol || !out_device || !points || !dirs || width <= 0 || width > 32768 || height <= 0) {
+        set_last_error("mk_render_cpr_noalloc: bad arguments");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (height > kNoAllocCprRows) {
+        set_last_error("mk_render_cpr_noalloc: height " + std::to_string(height) +
+                       " exceeds its fixed table of " + std::to_string(kNoAllocCprRows) + " rows");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &v = vol->st;
+    if (v.device < 0 || v.device >= kNoAllocMaxDevices) {
+        set_last_error("mk_render_cpr_noalloc: device index beyond the per-device table");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    MK_CUDA_TRY(cudaSetDevice(v.device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    // first call on this device: look up the array's device address (the
+    // host-side name of a __device__ variable is not a device pointer)
+    if (!g_noalloc_rows_dev[v.device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_cpr_rows);
+        if (e != cudaSuccess || !ptr) {
+            set_last_error(std::string("mk_render_cpr_noalloc: cudaGetSymbolAddress: ") +
+                           cudaGetErrorString(e));
+            return MK_ERR_CUDA;
+        }
+        g_noalloc_rows_dev[v.device] = ptr;
+    }
+    CprRow *d_rows = static_cast<CprRow *>(g_noalloc_rows_dev[v.device]);
+    for (int y = 0; y < height; ++y) {
+        for (int k = 0; k < 3; ++k) {
+            const double p = points[3 * y + k], d = dirs[3 * y + k];
+            CprRow &r = g_noalloc_rows_host[y];
+            r.p_hi[k] = (float)p;
+            r.p_lo[k] = (float)(p - (double)r.p_hi[k]);
+            r.d_hi[k] = (float)d;
+            r.d_lo[k] = (float)(d - (double)r.d_hi[k]);
+        }
+    }
+    // pageable source: the call returns once the rows are staged, so the host
+    // table may be refilled by the next call
+    MK_CUDA_TRY(cudaMemcpyAsync(d_rows, g_noalloc_rows_host, (size_t)height * sizeof(CprRow),
+                                cudaMemcpyHostToDevice, s));
+    dim3 grid((width + 31) / 32, (height + 7) / 8);
+    const float3 fdim = make_float3((float)v.dims[0], (float)v.dims[1], (float)v.dims[2]);
+    k_cpr<<<grid, 256, 0, s>>>(width, height, fdim, invert_z ? 1 : 0, d_rows, v.tex_linear, out_device);
+    MK_CUDA_TRY(cudaGetLastError());
+    return MK_OK;
 }
