@@ -39,8 +39,14 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "VR fps & Gsamples/s vs ref CUDA on 1xB200; served p50/p99 ms; bwd/fwd time"
-WORKLOAD = ("body VR: int16 512x512x1559 (0.7422x0.7422x1.0 mm), 4 labelled objects + background "
-            "(cap 0.4), 256-entry LUT per label, 1024x1024 RGB8, 36 views about z")
+WORKLOADS = {
+    "body": ("body VR: int16 512x512x1559 (0.7422x0.7422x1.0 mm), 4 labelled objects + background "
+             "(cap {bg}), 256-entry LUT per label, {size}x{size} RGB8, 36 views about z"),
+    "cardiac": ("cardiac VR: int16 512x512x361 (0.351x0.351x0.3 mm), one 256-entry LUT, "
+                "{size}x{size} RGB8, 36 views about z"),
+    "small": ("small VR: int16 128x128x96 (0.35x0.35x0.3 mm), one 256-entry LUT, {size}x{size} RGB8, "
+              "3 views about z"),
+}
 
 
 def parse_args():
@@ -50,6 +56,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["mine", "reference"], default="mine")
     ap.add_argument("--bg", type=float, default=0.4)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="body")
     ap.add_argument("--size", type=int, default=1024)
     ap.add_argument("--suite", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -227,7 +234,7 @@ def run_mine(args, rank, local, world):
     from monkeygl_b200 import capi
     from monkeygl_b200.workloads import make_workload
 
-    w = make_workload("body", bg_alpha=args.bg)
+    w = make_workload(args.workload, bg_alpha=args.bg)
     size = args.size
     vol = setup_volume(w, local)
     angles = w.angles
@@ -281,7 +288,8 @@ def run_mine(args, rank, local, world):
     # reference-schedule samples per frame (all views) and footprint bytes (3 views)
     samples = [vol.count_samples(p) for p in params]
     mean_samples = float(np.mean(samples))
-    foot = [vol.count_footprint(params[i]) for i in (0, 12, 24)]
+    n = len(params)
+    foot = [vol.count_footprint(params[i]) for i in sorted({0, n // 3, (2 * n) // 3})]
     vox = float(np.mean([f[1] for f in foot]))
     lab = float(np.mean([f[2] for f in foot]))
     out_bytes = size * size * 3
@@ -295,7 +303,7 @@ def run_mine(args, rank, local, world):
         "metric": METRIC, "value": round(value, 3), "unit": "fps", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": round(total_max * 1e3 / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "views": len(angles), "image": f"{size}x{size}",
+        "config": {"workload": WORKLOADS[args.workload].format(bg=args.bg, size=size), "views": len(angles), "image": f"{size}x{size}",
                    "bg_alpha": args.bg, "l2": "flushed between steps (256 MiB write, outside the events)",
                    "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
         "gsamples_per_s": round(gsps * world, 3),
@@ -330,7 +338,7 @@ def run_reference(args, rank, world):
         return None
     if not oracle.ref_gpu_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libmkref_gpu.so was not built"}
-    w = make_workload("body", bg_alpha=args.bg)
+    w = make_workload(args.workload, bg_alpha=args.bg)
     size = args.size
     ref = oracle.RefGPU()
     ref.set_volume(w.phantom.volume)
@@ -353,13 +361,14 @@ def run_reference(args, rank, world):
         ref.render_into(out, size, size, 0, flats[i % len(flats)])
     dt = time.perf_counter() - t0
     clk = clocks.stop()
-    kms = float(np.mean([ref.kernel_ms(size, size, 0, flats[i], 3) for i in (0, 9, 18, 27)]))
+    kms = float(np.mean([ref.kernel_ms(size, size, 0, flats[i], 3)
+                         for i in sorted({(k * len(flats)) // 4 for k in range(4)})]))
     value = K / dt
     return {
         "metric": METRIC, "impl": "reference", "value": round(value, 3), "unit": "fps", "n_gpus": 1,
         "steps": K, "warmup": W, "ms_per_step": round(dt * 1e3 / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "views": len(w.angles), "image": f"{size}x{size}",
+        "config": {"workload": WORKLOADS[args.workload].format(bg=args.bg, size=size), "views": len(w.angles), "image": f"{size}x{size}",
                    "bg_alpha": args.bg, "l2": "inputs larger than L2 (817 MB volume)",
                    "parallelism": "single GPU"},
         "kernel_ms_per_frame": round(kms, 4),
