@@ -84,7 +84,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or jobs or not lib.exists() or lib.stat().st_mtime < _newest(objs):
         tmp = lib.with_suffix(".so.tmp")
         cmd = [NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", str(tmp)] + \
-              [str(o) for o in objs] + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+              [str(o) for o in objs] + ["-lcudart_static", "-lrt", "-lpthread", "-ldl", "-lz"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
