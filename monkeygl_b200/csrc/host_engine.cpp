@@ -983,8 +983,9 @@ void Engine::UpdateCPRInfo() {
         z = start.z() - n.x() / n.z();
     }
     const Direction3d first(start, Point3d(x, y, z));
-    cprOriginStretched_ = start + first * cprStretchedRadius_;
-    cprOriginStraightened_ = start + first * cprStraightenedRadius_;
+    // MonkeyGL reads both radii through float getters (core/CPRInfo.h)
+    cprOriginStretched_ = start + first * (double)(float)cprStretchedRadius_;
+    cprOriginStraightened_ = start + first * (double)(float)cprStraightenedRadius_;
     cprAngleStretched_ = 0;
     cprAngleStraightened_ = 0;
 }
@@ -1005,7 +1006,7 @@ bool Engine::SetCPRLinePatient(const std::vector<Point3d> &line) {
 
 bool Engine::CPRStretched(std::vector<Point3d> &pts, std::vector<Direction3d> &dirs, int &w, int &h) const {
     if (cprLine_.size() < 2) return false;
-    w = cprStretchedRadius_ * 2.0 + 1;
+    w = (float)cprStretchedRadius_ * 2.0 + 1;
     if (w % 2) w += 1;
     const Point3d start = cprLine_.front();
     const Point3d rot = rotate_point(cprOriginStretched_, cprDirStretched_, start, cprAngleStretched_ * PI / 180.0);
@@ -1027,7 +1028,7 @@ bool Engine::CPRStretched(std::vector<Point3d> &pts, std::vector<Direction3d> &d
 
 bool Engine::CPRStraightened(std::vector<Point3d> &pts, std::vector<Direction3d> &dirs, int &w, int &h) const {
     if (cprLine_.size() < 2) return false;
-    w = cprStraightenedRadius_ * 2.0 + 1;
+    w = (float)cprStraightenedRadius_ * 2.0 + 1;
     if (w % 2) w += 1;
     h = (int)cprLine_.size();
     pts.assign(h, Point3d());          // the last row keeps its default (origin, +x)
