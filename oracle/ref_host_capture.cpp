@@ -41,6 +41,11 @@ void push3(std::vector<double> &v, float3 f) {
 
 }  // namespace
 
+// Built with -DMKREF_FULL (oracle/Makefile target ref-full) the stand-ins
+// below are left out and MonkeyGL's own core/kernel.cu and
+// core/CuDataManager.cu provide the launchers: the same driver then runs
+// MonkeyGL's complete HelloMonkey path on the GPU.
+#ifndef MKREF_FULL
 extern "C" void cu_copyVolumeData(short *, cudaExtent, cudaArray *&, cudaTextureObject_t &) {}
 extern "C" void cu_copyMaskData(unsigned char *, cudaExtent, cudaArray *&, cudaTextureObject_t &) {}
 extern "C" void cu_setTransferFunc(float *, int, cudaArray *&, cudaTextureObject_t &) {}
@@ -131,6 +136,8 @@ extern "C" void cu_renderCPR(short *pData, int width, int height, cudaTextureObj
     for (int i = 0; i < 3 * height; ++i) v.push_back(dirs[i]);
     memset(pData, 0, (size_t)width * height * sizeof(short));
 }
+
+#endif  // MKREF_FULL
 
 // ------------------------------------------------------------------------
 // Driver ABI.  HelloMonkey's constructor loads ./resources/human.stl
@@ -247,6 +254,46 @@ extern "C" int mkrh_get_plane(void *h, int plane, int *wh) {
     if (!ok) return 0;
     return (int)(plane >= (int)PlaneStretchedCPR ? cap.cpr.size() : cap.plane.size());
 }
+// SetTransferFunc(rgb points[, alpha points], label); label < 0 = active label.
+extern "C" int mkrh_set_tf(void *h, const int *rgb_pos, const float *rgba, int n_rgb, const int *a_pos,
+                           const float *alpha, int n_alpha, int label) {
+    std::map<int, RGBA> rgb;
+    for (int i = 0; i < n_rgb; ++i)
+        rgb[rgb_pos[i]] = RGBA(rgba[4 * i], rgba[4 * i + 1], rgba[4 * i + 2], rgba[4 * i + 3]);
+    std::map<int, float> al;
+    for (int i = 0; i < n_alpha; ++i) al[a_pos[i]] = alpha[i];
+    bool ok;
+    if (n_alpha > 0)
+        ok = label < 0 ? HM->SetTransferFunc(rgb, al) : HM->SetTransferFunc(rgb, al, (unsigned char)label);
+    else
+        ok = label < 0 ? HM->SetTransferFunc(rgb) : HM->SetTransferFunc(rgb, (unsigned char)label);
+    return ok ? 1 : 0;
+}
+
+// GetVRData into `out` (capacity `cap_bytes`); wh receives the image size.
+extern "C" int mkrh_vr_image(void *h, unsigned char *out, long long cap_bytes, int *wh) {
+    std::shared_ptr<unsigned char> p;
+    int w = 0, hh = 0;
+    HM->GetPlaneMaxSize(w, hh, PlaneVR);
+    wh[0] = w;
+    wh[1] = hh;
+    if (!HM->GetVRData(p, w, hh) || !p || (long long)w * hh * 3 > cap_bytes) return 0;
+    memcpy(out, p.get(), (size_t)w * hh * 3);
+    return 1;
+}
+
+// GetPlaneData into `out` (capacity in values); wh receives the plane size.
+extern "C" int mkrh_plane_image(void *h, int plane, short *out, long long cap_values, int *wh) {
+    std::shared_ptr<short> p;
+    int w = 0, hh = 0;
+    bool ok = HM->GetPlaneData(p, w, hh, (PlaneType)plane);
+    wh[0] = w;
+    wh[1] = hh;
+    if (!ok || !p || (long long)w * hh > cap_values) return 0;
+    memcpy(out, p.get(), (size_t)w * hh * sizeof(short));
+    return 1;
+}
+
 extern "C" int mkrh_plane_kind(void) { return cap.plane_type; }
 extern "C" void mkrh_copy_vr(double *out) { memcpy(out, cap.vr.data(), cap.vr.size() * sizeof(double)); }
 extern "C" void mkrh_copy_plane(double *out) { memcpy(out, cap.plane.data(), cap.plane.size() * sizeof(double)); }
