@@ -5,6 +5,7 @@
 // the camera matrices, label windows, plane frames and CPR frames produced by
 // MonkeyGL's own HelloMonkey API can be read back on a machine without a GPU.
 // tests/golden/make_host_golden.py drives this through the mkrh_* functions.
+#include <malloc.h>
 #include <string.h>
 #include <unistd.h>
 
@@ -16,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "CuDataManager.h"
+#include "DataManager.h"
 #include "Defines.h"
 #include "HelloMonkey.h"
 #include "TransferFunction.h"
@@ -143,6 +145,19 @@ extern "C" void cu_renderCPR(short *pData, int width, int height, cudaTextureObj
 // Driver ABI.  HelloMonkey's constructor loads ./resources/human.stl
 // (core/MarchingCube.cpp:298), so mkrh_create takes the directory that holds
 // resources/ and constructs the object from there.
+
+// mkrh_zero_heap(1) makes every allocation of 64 KiB or more come from fresh
+// (zero-filled) pages.  MonkeyGL's VolumeInfo::AddNewObjectMask allocates the
+// label volume with new[] and never clears it (core/VolumeInfo.cpp:96-104);
+// recycled heap memory there leaves labels above 64 outside every mask, which
+// its kernel then uses to index 65-entry tables.  With fresh pages the label
+// volume starts at zero, as MonkeyGL evidently assumes.
+extern "C" int mkrh_zero_heap(int on) {
+    return on ? mallopt(M_MMAP_THRESHOLD, 64 * 1024) : 1;
+}
+
+// Largest label in MonkeyGL's stored label volume (-1 if there is none).
+extern "C" int mkrh_mask_max_label(void *h);
 
 extern "C" void *mkrh_create(const char *asset_dir) {
     char cwd[4096];
@@ -292,6 +307,18 @@ extern "C" int mkrh_plane_image(void *h, int plane, short *out, long long cap_va
     if (!ok || !p || (long long)w * hh > cap_values) return 0;
     memcpy(out, p.get(), (size_t)w * hh * sizeof(short));
     return 1;
+}
+
+extern "C" int mkrh_mask_max_label(void *h) {
+    int w = 0, hh = 0, d = 0;
+    HM->GetVolumeData(w, hh, d);
+    // HelloMonkey exposes no mask accessor; IRender's GetMaskData is reached
+    // through the DataManager that every instance shares
+    std::shared_ptr<unsigned char> m = DataManager::Instance()->GetMaskData();
+    if (!m) return -1;
+    int mx = 0;
+    for (size_t i = 0; i < (size_t)w * hh * d; ++i) mx = m.get()[i] > mx ? m.get()[i] : mx;
+    return mx;
 }
 
 extern "C" int mkrh_plane_kind(void) { return cap.plane_type; }

@@ -54,6 +54,10 @@ class RefHelloMonkey:
             }
             for f, a in sig.items():
                 getattr(L, f).argtypes = a
+            L.mkrh_mask_max_label.argtypes = [vp]
+            # MonkeyGL allocates its label volume uncleared (core/VolumeInfo.cpp:96-104);
+            # fresh zero pages keep labels outside the masks at 0
+            assert L.mkrh_zero_heap(1) == 1
             RefHelloMonkey.L = L
             RefHelloMonkey.h = L.mkrh_create(str(FULL.parent).encode())
         self.L, self.h = RefHelloMonkey.L, RefHelloMonkey.h
@@ -80,6 +84,9 @@ def run_both(p, ops, masks=None):
         a = L.mkrh_add_mask(h, ptr(m), X, Y, Z)
         b = mine.AddNewObjectMaskArray(m.swapaxes(2, 0))
         assert a == b
+    if masks:
+        # never hand MonkeyGL's kernel a label beyond its 65-entry tables
+        assert 0 <= L.mkrh_mask_max_label(h) <= len(masks)
     orient = [mine.Anterior, mine.Posterior, mine.Left, mine.Right, mine.Head, mine.Foot]
     for op in [("orientation", 0), ("reset",), ("vr_size", 512, 512), ("render_type", 0), ("mpr_type", 0),
                ("background", 0.0, 0.0, 0.0, 0.0)] + list(ops):
@@ -170,6 +177,18 @@ def phantom():
 TF4 = {0: (0.9, 0.3, 0.2, 0.0), 22: (0.95, 0.4, 0.3, 0.0), 55: (0.9, 0.7, 0.5, 0.35), 99: (1.0, 0.95, 0.9, 0.85)}
 
 
+# MonkeyGL keeps one process-wide state: SetVolumeData clears its host-side
+# labels but not the device label texture nor the per-label window table of
+# the previous volume (core/DataManager.cpp:144-165).  This test needs that
+# state fresh, so it runs first; later tests set every window they use.
+def test_default_windows_render_background(phantom):
+    # before any SetVRWWWL / SetObjectAlpha every label's cap is 0
+    ref, mine = run_both(phantom, [("tf", TF4, {}, -1), ("background", 0.2, 0.3, 0.4, 1.0)])
+    img = mine.GetVRImage()
+    assert_vr_equal(img, ref_vr(ref), "default windows")
+    assert (img[:200, :200] == [51, 76, 102]).all()
+
+
 @pytest.mark.parametrize("rtype", [0, 1, 2])
 def test_vr_through_the_api(phantom, rtype):
     ops = [("tf", TF4, {}, -1), ("wwwl", 1700, 650, -1), ("render_type", rtype), ("rotate", 30, 10),
@@ -188,14 +207,6 @@ def test_multilabel_vr_through_the_api(phantom):
            ("rotate", 60, 0), ("vr_size", 640, 480)]
     ref, mine = run_both(phantom, ops, masks)
     assert_vr_equal(mine.GetVRImage(), ref_vr(ref), "multi-label VR")
-
-
-def test_default_windows_render_background(phantom):
-    # before any SetVRWWWL / SetObjectAlpha every label's cap is 0
-    ref, mine = run_both(phantom, [("tf", TF4, {}, -1), ("background", 0.2, 0.3, 0.4, 1.0)])
-    img = mine.GetVRImage()
-    assert_vr_equal(img, ref_vr(ref), "default windows")
-    assert (img[:200, :200] == [51, 76, 102]).all()
 
 
 def test_planes_through_the_api(phantom):
