@@ -234,6 +234,49 @@ int mk_render_cpr(mk_volume vol, int width, int height, const double *points,
                   const double *dirs, int invert_z, int16_t *out, int out_on_device,
                   void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Differentiable volume rendering (no counterpart in MonkeyGL)        */
+/* ------------------------------------------------------------------ */
+
+/*
+ * MonkeyGL's orthographic VR camera (the pixel -> ray mapping of
+ * core/kernel.cu:161-206) with a differentiable method: fixed step, float32
+ * volume in [0,1] (x-fastest, dims[0]*dims[1]*dims[2]) sampled with exact
+ * trilinear weights, the value used directly as the LUT coordinate
+ * (lut_len float4 entries, linear, clamp), front-to-back compositing stopped
+ * once transmittance falls below t_min.  All pointers are device pointers;
+ * calls are asynchronous on `stream`.
+ */
+typedef struct mk_dvr_params {
+    int width;
+    int height;
+    int dims[3];
+    float max_len_spacing[3];
+    float transform[9];
+    float scale;
+    float x_translate;
+    float y_translate;
+    float step;                  /* in MonkeyGL's ray parameter: 1/dim_z is one voxel of the longest axis */
+    float t_min;                 /* early termination threshold on transmittance (0 = never) */
+    int lut_len;                 /* 2..1024 */
+} mk_dvr_params;
+
+/* Floats of workspace mk_dvr_forward needs to support a backward pass
+ * (per-ray transmittance checkpoints and sample counts). */
+int mk_dvr_workspace_floats(const mk_dvr_params *params, size_t *floats);
+
+/* image: width*height*3 floats (RGB); transmittance: width*height floats;
+ * workspace: mk_dvr_workspace_floats floats, or NULL for inference only. */
+int mk_dvr_forward(const mk_dvr_params *params, const float *volume, const float *lut, float *image,
+                   float *transmittance, float *workspace, void *stream);
+
+/* Accumulates (adds) dL/dLUT into grad_lut (lut_len*4 floats) and, when
+ * grad_volume is not NULL, dL/dvolume into grad_volume, given grad_image =
+ * dL/dimage and the workspace of the matching forward call. */
+int mk_dvr_backward(const mk_dvr_params *params, const float *volume, const float *lut,
+                    const float *workspace, const float *grad_image, float *grad_lut,
+                    float *grad_volume, void *stream);
+
 /*
  * mk_render_cpr without any device allocation.  It has no counterpart in
  * MonkeyGL: it is for callers that cannot call cudaMalloc (a host with a

@@ -642,3 +642,81 @@ int mko_render_cpr(const mko_volume *v, int w, int h, const double *pts, const d
     (void)nthreads;
     return 0;
 }
+
+/* ---------------------------------------------------------------- */
+/* differentiable VR (the method of monkeygl_b200/csrc/mk_dvr.cu) in FP64 */
+
+/* p: [0] w, [1] h, [2..4] dims, [5..7] maxLenSpacing, [8..16] camera matrix,
+ * [17] scale, [18] xT, [19] yT, [20] step, [21] t_min, [22] lut_len.
+ * vol: dims[0]*dims[1]*dims[2] doubles (x fastest); lut: lut_len*4 doubles;
+ * image: w*h*3 doubles. */
+int mko_dvr_forward_d(const double *p, const double *vol, const double *lut, int nthreads, double *image) {
+    const int w = (int)p[0], h = (int)p[1];
+    const int dim[3] = {(int)p[2], (int)p[3], (int)p[4]};
+    const double *mls = p + 5, *M = p + 8;
+    const double scale = p[17], xT = p[18], yT = p[19], step = p[20], t_min = p[21];
+    const int n_lut = (int)p[22];
+    if (w <= 0 || h <= 0 || dim[0] <= 0 || dim[1] <= 0 || dim[2] <= 0 || n_lut < 2 || !(step > 0)) return 1;
+#ifdef _OPENMP
+    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+#endif
+    for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < w; ++x) {
+            const double u = (x - w / 2.0 - xT) / h, v = (y - h / 2.0 - yT) / h;
+            double base[3], dir[3], lo = 0.0, hi = 1.732;
+            int hit = 1;
+            for (int k = 0; k < 3; ++k) {
+                base[k] = (M[3 * k] * u + M[3 * k + 1] * (-0.866 * scale) + M[3 * k + 2] * v) * mls[k] + 0.5;
+                dir[k] = M[3 * k + 1] * scale * mls[k];
+                if (fabs(dir[k]) < 1e-12) {
+                    if (base[k] < 0.0 || base[k] > 1.0) hit = 0;
+                    continue;
+                }
+                double t0 = -base[k] / dir[k], t1 = (1.0 - base[k]) / dir[k];
+                if (t0 > t1) { double t = t0; t0 = t1; t1 = t; }
+                if (t0 > lo) lo = t0;
+                if (t1 < hi) hi = t1;
+            }
+            double C[3] = {0, 0, 0}, T = 1.0;
+            if (hit && lo < hi) {
+                const double a0 = ceil(lo / step) * step;
+                const int n = (int)floor((hi - a0) / step) + 1;
+                for (int i = 0; i < n; ++i) {
+                    const double a = a0 + i * step;
+                    double c[3], fr[3];
+                    int i0[3];
+                    for (int k = 0; k < 3; ++k) {
+                        c[k] = (base[k] + a * dir[k]) * dim[k] - 0.5;
+                        double f = floor(c[k]);
+                        i0[k] = (int)f;
+                        fr[k] = c[k] - f;
+                    }
+                    double s = 0.0;
+                    for (int dz = 0; dz < 2; ++dz)
+                        for (int dy = 0; dy < 2; ++dy)
+                            for (int dx = 0; dx < 2; ++dx) {
+                                int ix = clampi(i0[0] + dx, 0, dim[0] - 1);
+                                int iy = clampi(i0[1] + dy, 0, dim[1] - 1);
+                                int iz = clampi(i0[2] + dz, 0, dim[2] - 1);
+                                double wt = (dx ? fr[0] : 1 - fr[0]) * (dy ? fr[1] : 1 - fr[1]) * (dz ? fr[2] : 1 - fr[2]);
+                                s += wt * vol[((size_t)iz * dim[1] + iy) * dim[0] + ix];
+                            }
+                    double xx = s * n_lut - 0.5, f = floor(xx), wgt = xx - f;
+                    int k = (int)f, k0, k1;
+                    if (k < 0) { k0 = k1 = 0; wgt = 0; }
+                    else if (k >= n_lut - 1) { k0 = k1 = n_lut - 1; wgt = 0; }
+                    else { k0 = k; k1 = k + 1; }
+                    double q[4];
+                    for (int ch = 0; ch < 4; ++ch) q[ch] = lut[4 * k0 + ch] + wgt * (lut[4 * k1 + ch] - lut[4 * k0 + ch]);
+                    for (int ch = 0; ch < 3; ++ch) C[ch] += T * q[3] * q[ch];
+                    T *= 1.0 - q[3];
+                    if (T < t_min) break;
+                }
+            }
+            for (int ch = 0; ch < 3; ++ch) image[((size_t)y * w + x) * 3 + ch] = C[ch];
+        }
+    }
+    (void)nthreads;
+    return 0;
+}

@@ -76,6 +76,13 @@ int mko_render_plane(const mko_volume *v, int w, int h, const float *params, int
 int mko_render_cpr(const mko_volume *v, int w, int h, const double *pts, const double *dirs,
                    int invert_z, int precision, int nthreads, int16_t *out);
 
+/* The differentiable method of monkeygl_b200/csrc/mk_dvr.cu in FP64 (for
+ * central finite differences).  p: [0] width, [1] height, [2..4] dims,
+ * [5..7] maxLenSpacing, [8..16] camera matrix, [17] scale, [18] xT, [19] yT,
+ * [20] step, [21] t_min, [22] lut_len; vol and lut are doubles; image is
+ * width*height*3 doubles. */
+int mko_dvr_forward_d(const double *p, const double *vol, const double *lut, int nthreads, double *image);
+
 /* Single texture fetches, exposed for known-answer tests. */
 float mko_tex3d_linear(const mko_volume *v, float x, float y, float z);
 float mko_tex3d_point(const mko_volume *v, float x, float y, float z);

@@ -1,0 +1,222 @@
+"""Differentiable volume rendering: forward against the FP64 restatement,
+hand-written gradients against FP64 central finite differences and against
+torch autograd over a materialised sample tensor.
+
+Sizes are reduced so the FP64 CPU evaluations stay in seconds: a 64^3
+float32 phantom in [0, 1], 64x64 images, two views, step 0.5 voxel.  The
+full-size timing (256^3, 8 views of 256^2) is in bench.py --suite."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from monkeygl_b200 import dvr
+from monkeygl_b200.camera import view_camera
+from monkeygl_b200.phantom import make_phantom, make_tf_control_points, make_tf_lut
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def oracle_forward(p, vol64, lut64):
+    L = oracle.cpu()
+    L.mko_dvr_forward_d.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    out = np.zeros((p.height, p.width, 3), np.float64)
+    flat = dvr.params_flat(p)
+    rc = L.mko_dvr_forward_d(C.c_void_p(flat.ctypes.data), C.c_void_p(vol64.ctypes.data),
+                             C.c_void_p(lut64.ctypes.data), 0, C.c_void_p(out.ctypes.data))
+    assert rc == 0
+    return out
+
+
+@pytest.fixture(scope="module")
+def setup():
+    ph = make_phantom((64, 64, 64), (1.0, 1.0, 1.0), 77)
+    vol = np.clip((ph.volume.astype(np.float32) + 1024.0) / 4095.0, 0.0, 1.0).astype(np.float32)
+    rng = np.random.Generator(np.random.PCG64(5))
+    # LUT over the normalised value: soft tissue (~0.26) transparent, dense values opaque
+    lut = make_tf_lut(make_tf_control_points(rng))
+    target_lut = make_tf_lut(make_tf_control_points(rng))
+    views = [dvr.dvr_params(64, 64, view_camera(a), (64, 64, 64), (1, 1, 1), 0.5, 0.0, 256) for a in (0.0, 50.0)]
+    return vol, lut, target_lut, views
+
+
+def loss_fd(vol64, lut64, views, targets):
+    total = 0.0
+    for p, t in zip(views, targets):
+        img = oracle_forward(p, vol64, lut64)
+        total += ((img - t) ** 2).sum()
+    return total
+
+
+def test_forward_matches_fp64(setup):
+    vol, lut, _, views = setup
+    v = torch.tensor(vol, device="cuda")
+    l = torch.tensor(lut, device="cuda")
+    imgs = dvr.render(v, l, views).cpu().numpy()
+    for i, p in enumerate(views):
+        ref = oracle_forward(p, vol.astype(np.float64), lut.astype(np.float64))
+        err = np.abs(imgs[i] - ref).max()
+        print(f"view {i}: max |fp32 - fp64| = {err:.2e}, image max {ref.max():.3f}")
+        assert err < 2e-4
+        assert ref.max() > 0.05     # something was rendered
+
+
+def test_gradients_match_fp64_finite_differences(setup):
+    vol, lut, target_lut, views = setup
+    v = torch.tensor(vol, device="cuda", requires_grad=True)
+    l = torch.tensor(lut, device="cuda", requires_grad=True)
+    with torch.no_grad():
+        targets = dvr.render(v, torch.tensor(target_lut, device="cuda"), views)
+    imgs = dvr.render(v, l, views)
+    loss = ((imgs - targets) ** 2).sum()
+    loss.backward()
+    g_lut = l.grad.cpu().numpy().astype(np.float64)
+    g_vol = v.grad.cpu().numpy().astype(np.float64)
+    t64 = [t.cpu().numpy().astype(np.float64) for t in targets]
+    vol64, lut64 = vol.astype(np.float64), lut.astype(np.float64)
+    rng = np.random.default_rng(9)
+    # The image is a polynomial in the LUT entries, but of high degree: the
+    # entry that air maps to is met by ~128 samples per ray, so the loss holds
+    # (1 - a)^128 and a central difference at 1e-3 is off by eps^2 f'''/6,
+    # about 0.3-1% for that entry.  1e-5 brings this below 1e-6.
+    eps = 1e-5
+    # 64 random LUT entries among those the rays reach, plus the air entry
+    live = np.argwhere(np.abs(g_lut) > 1e-6 * np.abs(g_lut).max())
+    pick = live[rng.choice(len(live), size=min(64, len(live)), replace=False)]
+    pick = np.concatenate([pick, np.array(np.unravel_index(np.argmax(np.abs(g_lut)), g_lut.shape))[None, :]])
+    # entry 0: the phantom's lowest value (-1000 HU) maps past it, gradient 0
+    pick = np.concatenate([pick, [[0, 3]]])
+    fd, an = [], []
+    for (k, ch) in pick:
+        lp, lm = lut64.copy(), lut64.copy()
+        lp[k, ch] += eps
+        lm[k, ch] -= eps
+        fd.append((loss_fd(vol64, lp, views, t64) - loss_fd(vol64, lm, views, t64)) / (2 * eps))
+        an.append(g_lut[k, ch])
+    fd, an = np.array(fd), np.array(an)
+    rel = np.linalg.norm(fd - an) / np.linalg.norm(fd)
+    print(f"LUT: {len(fd)} entries, relative error {rel:.2e}, worst entry {np.max(np.abs(fd - an) / np.abs(fd).max()):.2e}")
+    assert rel <= 1e-3
+    # 64 random voxels among those with a gradient.  The loss is only
+    # piecewise smooth in a voxel value: the LUT is piecewise linear, and its
+    # slope changes at the transfer function's control points.  The phantom's
+    # soft tissue (~0.26) sits on the first control point (0.18-0.28), and a
+    # step of 1e-3 moves a sample's LUT coordinate by up to 0.256 entries, so
+    # central differences at 1e-3 straddle the kink: 2.8e-2 relative error.
+    # At 1e-5 the ~2000 samples behind these 64 voxels still hold a few that
+    # cross a control point (6e-3); at 1e-7 the chance of one is about 1%,
+    # while FP64 rounding in the difference stays near 1e-6 relative.
+    eps = 1e-7
+    live = np.argwhere(np.abs(g_vol) > 1e-4 * np.abs(g_vol).max())
+    pick = live[rng.choice(len(live), size=min(64, len(live)), replace=False)]
+    fd, an = [], []
+    for (z, y, x) in pick:
+        vp, vm = vol64.copy(), vol64.copy()
+        vp[z, y, x] += eps
+        vm[z, y, x] -= eps
+        fd.append((loss_fd(vp, lut64, views, t64) - loss_fd(vm, lut64, views, t64)) / (2 * eps))
+        an.append(g_vol[z, y, x])
+    fd, an = np.array(fd), np.array(an)
+    rel = np.linalg.norm(fd - an) / np.linalg.norm(fd)
+    print(f"voxels: {len(fd)} entries, relative error {rel:.2e}")
+    assert rel <= 1e-3
+
+
+def torch_reference(vol, lut, p, counts):
+    """The same method with autograd over a materialised (rays, samples) tensor."""
+    W, H = p.width, p.height
+    dims = list(p.dims)
+    M = torch.tensor(list(p.transform), dtype=torch.float32, device="cuda").view(3, 3)
+    mls = torch.tensor(list(p.max_len_spacing), dtype=torch.float32, device="cuda")
+    ys, xs = torch.meshgrid(torch.arange(H, device="cuda"), torch.arange(W, device="cuda"), indexing="ij")
+    u = ((xs.float() - W / 2.0) - p.x_translate) / H
+    v = ((ys.float() - H / 2.0) - p.y_translate) / H
+    uvw = torch.stack([u, torch.full_like(u, -0.866 * p.scale), v], -1)          # (H, W, 3)
+    base = (uvw @ M.T) * mls + 0.5
+    direc = (M[:, 1] * p.scale) * mls
+    lo = torch.zeros_like(u)
+    hi = torch.full_like(u, 1.732)
+    for k in range(3):
+        # a ray parallel to a pair of faces is not clipped by them (as in the
+        # kernel); dividing by the zero component would give 0/0 on a face
+        if abs(direc[k].item()) < 1e-12:
+            continue
+        t0 = (0.0 - base[..., k]) / direc[k]
+        t1 = (1.0 - base[..., k]) / direc[k]
+        lo = torch.maximum(lo, torch.minimum(t0, t1))
+        hi = torch.minimum(hi, torch.maximum(t0, t1))
+    a0 = torch.ceil(lo / p.step) * p.step
+    nmax = int(counts.max())
+    i = torch.arange(nmax, device="cuda", dtype=torch.float32)
+    a = a0[..., None] + i * p.step                                                # (H, W, n)
+    valid = (torch.arange(nmax, device="cuda")[None, None, :] < counts[..., None])
+    pos = base[..., None, :] + a[..., None] * direc                               # (H, W, n, 3)
+    dimsf = torch.tensor(dims, dtype=torch.float32, device="cuda")
+    c = pos * dimsf - 0.5
+    f = torch.floor(c)
+    w = c - f
+    i0 = f.long()
+    s = 0
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                ix = (i0[..., 0] + dx).clamp(0, dims[0] - 1)
+                iy = (i0[..., 1] + dy).clamp(0, dims[1] - 1)
+                iz = (i0[..., 2] + dz).clamp(0, dims[2] - 1)
+                wt = (w[..., 0] if dx else 1 - w[..., 0]) * (w[..., 1] if dy else 1 - w[..., 1]) * \
+                     (w[..., 2] if dz else 1 - w[..., 2])
+                s = s + wt * vol[iz, iy, ix]
+    n = lut.shape[0]
+    xq = s * n - 0.5
+    fq = torch.floor(xq)
+    kq = fq.long()
+    inside = (kq >= 0) & (kq < n - 1)
+    k0 = torch.where(kq < 0, 0, torch.where(kq >= n - 1, n - 1, kq))
+    k1 = torch.where(inside, kq + 1, k0)
+    wq = torch.where(inside, xq - fq, torch.zeros_like(xq))
+    q = lut[k0] + wq[..., None] * (lut[k1] - lut[k0])                            # (H, W, n, 4)
+    alpha = q[..., 3] * valid
+    T = torch.cumprod(torch.cat([torch.ones_like(alpha[..., :1]), 1 - alpha[..., :-1]], -1), -1)
+    return (T[..., None] * alpha[..., None] * q[..., :3]).sum(-2)
+
+
+def test_gradients_match_torch_autograd(setup):
+    vol, lut, target_lut, views = setup
+    target = torch.rand((64, 64, 3), device="cuda")
+    for p in views:
+        v = torch.tensor(vol, device="cuda", requires_grad=True)
+        l = torch.tensor(lut, device="cuda", requires_grad=True)
+        img = dvr.render(v, l, [p])[0]
+        ((img - target) ** 2).sum().backward()
+        # sample counts per ray from the kernel's workspace
+        L = dvr._lib()
+        nws = C.c_size_t(0)
+        L.mk_dvr_workspace_floats(C.byref(p), C.byref(nws))
+        work = torch.empty(nws.value, dtype=torch.float32, device="cuda")
+        img2 = torch.empty((64, 64, 3), device="cuda")
+        tr = torch.empty((64, 64), device="cuda")
+        L.mk_dvr_forward(C.byref(p), C.c_void_p(v.data_ptr()), C.c_void_p(l.data_ptr()), C.c_void_p(img2.data_ptr()),
+                         C.c_void_p(tr.data_ptr()), C.c_void_p(work.data_ptr()), None)
+        torch.cuda.synchronize()
+        counts = work[-64 * 64:].view(torch.int32).view(64, 64)
+        v2 = torch.tensor(vol, device="cuda", requires_grad=True)
+        l2 = torch.tensor(lut, device="cuda", requires_grad=True)
+        ref = torch_reference(v2, l2, p, counts)
+        ((ref - target) ** 2).sum().backward()
+        assert (img - ref).abs().max().item() < 1e-4
+        for name, a, b in (("lut", l.grad, l2.grad), ("volume", v.grad, v2.grad)):
+            rel = ((a - b).norm() / b.norm()).item()
+            print(f"{name}: relative error vs torch autograd {rel:.2e}")
+            assert rel < 1e-3
+
+
+def test_invalid_parameters_are_rejected():
+    p = dvr.dvr_params(8, 8, view_camera(0.0), (4, 4, 4), (1, 1, 1))
+    p.lut_len = 1
+    v = torch.zeros((4, 4, 4), device="cuda")
+    l = torch.zeros((1, 4), device="cuda")
+    with pytest.raises(Exception):
+        dvr.render(v, l, [p])
