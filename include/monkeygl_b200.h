@@ -241,11 +241,13 @@ int mk_render_cpr(mk_volume vol, int width, int height, const double *points,
 /*
  * MonkeyGL's orthographic VR camera (the pixel -> ray mapping of
  * core/kernel.cu:161-206) with a differentiable method: fixed step, float32
- * volume in [0,1] (x-fastest, dims[0]*dims[1]*dims[2]) sampled with exact
- * trilinear weights, the value used directly as the LUT coordinate
- * (lut_len float4 entries, linear, clamp), front-to-back compositing stopped
- * once transmittance falls below t_min.  All pointers are device pointers;
- * calls are asynchronous on `stream`.
+ * volume in [0,1] (x-fastest, dims[0]*dims[1]*dims[2], fewer than 2^31
+ * voxels) sampled with exact trilinear weights (texel centres at
+ * (i+0.5)/dim, clamp to edge), the value used directly as the LUT coordinate
+ * (lut_len float4 entries, entry i centred at (i+0.5)/lut_len, linear,
+ * clamp), front-to-back compositing stopped after the sample that takes
+ * transmittance below t_min.  All pointers are device pointers; calls are
+ * asynchronous on `stream`.
  */
 typedef struct mk_dvr_params {
     int width;
@@ -261,20 +263,26 @@ typedef struct mk_dvr_params {
     int lut_len;                 /* 2..1024 */
 } mk_dvr_params;
 
+/* A call renders `nviews` views (any number; one launch per 32).  The views
+ * share width, height, dims and lut_len; the camera, spacing, scale,
+ * translation, step and t_min are per view. */
+
 /* Floats of workspace mk_dvr_forward needs to support a backward pass
  * (per-ray transmittance checkpoints and sample counts). */
-int mk_dvr_workspace_floats(const mk_dvr_params *params, size_t *floats);
+int mk_dvr_workspace_floats(const mk_dvr_params *views, int nviews, size_t *floats);
 
-/* image: width*height*3 floats (RGB); transmittance: width*height floats;
- * workspace: mk_dvr_workspace_floats floats, or NULL for inference only. */
-int mk_dvr_forward(const mk_dvr_params *params, const float *volume, const float *lut, float *image,
-                   float *transmittance, float *workspace, void *stream);
+/* images: nviews*height*width*3 floats (RGB); transmittance:
+ * nviews*height*width floats; workspace: mk_dvr_workspace_floats floats, or
+ * NULL for inference only. */
+int mk_dvr_forward(const mk_dvr_params *views, int nviews, const float *volume, const float *lut,
+                   float *images, float *transmittance, float *workspace, void *stream);
 
 /* Accumulates (adds) dL/dLUT into grad_lut (lut_len*4 floats) and, when
- * grad_volume is not NULL, dL/dvolume into grad_volume, given grad_image =
- * dL/dimage and the workspace of the matching forward call. */
-int mk_dvr_backward(const mk_dvr_params *params, const float *volume, const float *lut,
-                    const float *workspace, const float *grad_image, float *grad_lut,
+ * grad_volume is not NULL, dL/dvolume into grad_volume (dims floats, x
+ * fastest), given grad_images = dL/dimages and the workspace of the matching
+ * forward call. */
+int mk_dvr_backward(const mk_dvr_params *views, int nviews, const float *volume, const float *lut,
+                    const float *workspace, const float *grad_images, float *grad_lut,
                     float *grad_volume, void *stream);
 
 /*

@@ -65,6 +65,17 @@ class PlaneParams(C.Structure):
     ]
 
 
+
+class DVRParams(C.Structure):
+    """mk_dvr_params: one view of the differentiable renderer."""
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int), ("dims", C.c_int * 3),
+        ("max_len_spacing", C.c_float * 3), ("transform", C.c_float * 9),
+        ("scale", C.c_float), ("x_translate", C.c_float), ("y_translate", C.c_float),
+        ("step", C.c_float), ("t_min", C.c_float), ("lut_len", C.c_int),
+    ]
+
+
 _lib = None
 
 _SIGS = {
@@ -91,6 +102,9 @@ _SIGS = {
     "mk_render_cpr_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_void_p]),
     "mk_volume_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mk_dvr_workspace_floats": (C.c_int, [C.POINTER(DVRParams), C.c_int, C.POINTER(C.c_size_t)]),
+    "mk_dvr_forward": (C.c_int, [C.POINTER(DVRParams), C.c_int] + [C.c_void_p] * 6),
+    "mk_dvr_backward": (C.c_int, [C.POINTER(DVRParams), C.c_int] + [C.c_void_p] * 7),
 }
 
 

@@ -7,10 +7,13 @@
 // made differentiable: a fixed step along the ray (no adaptive refinement), a
 // float32 volume in [0, 1] sampled with exact trilinear weights (texel
 // centres at (i+0.5)/dim, clamp to edge), the value used directly as the LUT
-// coordinate (entry centres at (i+0.5)/n, linear interpolation, clamp), and
+// coordinate (entry i centred at (i+0.5)/n, linear interpolation, clamp), and
 // compositing
 //     C = sum_i T_i a_i c_i,   T_0 = 1,   T_{i+1} = T_i (1 - a_i),
 // stopped after the sample that takes T below t_min.  The image is C (RGB).
+// The texture unit is not used for the volume: its float32 trilinear filter
+// combines the x and y weights in fixed point below 8 fractional bits, so a
+// backward pass could not reproduce the weights of the forward one.
 //
 // Backward.  With g = dL/dC and U_i the colour composited behind sample i
 // seen from unit transmittance just after it (U_last = 0,
@@ -18,56 +21,67 @@
 //     dL/dc_i = T_i a_i g,     dL/da_i = T_i g . (c_i - U_i),
 // with no division by (1 - a_i).  T_i comes from per-ray checkpoints of T
 // every K samples: the backward walks segments of 16 samples from last to
-// first, re-marching each forward from its checkpoint into registers.
-// dL/dLUT goes through the interpolation weights into shared-memory bins
-// (warp-aggregated per bin, then one global atomic per bin and block);
-// dL/dvolume goes through the value's LUT slope and the trilinear weights
-// into eight global reductions per sample.
+// first, re-marching each forward from its checkpoint and keeping the sample
+// values and transmittances in registers.  A ray accumulates its dL/dLUT in
+// registers while its samples stay in one LUT cell and its dL/dvolume while
+// they stay in one voxel cell; a change of cell flushes the sums (shared-
+// memory bins for the LUT, eight global reductions for the voxels).
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #include "mk_internal.h"
 
 namespace mk {
 
 constexpr int kDvrMaxLut = 1024;
-constexpr int kDvrSeg = 16;          // samples per recomputed segment
-constexpr int kDvrMaxCkpt = 512;     // checkpoints per ray
+constexpr int kDvrSeg = 16;              // samples per recomputed segment
+constexpr int kDvrMaxCkpt = 512;         // checkpoints per ray
+constexpr int kDvrViewsPerLaunch = 32;
 
-struct DvrParams {
-    int W, H;
-    int dim[3];
-    float fdim[3];
-    float mls[3];
+struct DvrView {
     float M[9];
+    float mls[3];
     float scale, xT, yT;
     float step;
     float t_min;
-    int lut_len;
-    int ckpt;                        // samples between checkpoints (multiple of kDvrSeg)
+    int ckpt_shift;                      // samples between checkpoints = 1 << ckpt_shift (>= kDvrSeg)
     int max_ckpt;
+    unsigned long long work_off;         // floats from the workspace start
+};
+
+struct DvrBatch {
+    int W, H;
+    int lut_len;
+    int dim[3];
+    int sxy;                             // dim[0] * dim[1]
+    float fdim[3];
+    DvrView v[kDvrViewsPerLaunch];
 };
 
 struct Ray {
-    float px, py, pz;                // normalized position at a = 0
-    float dx, dy, dz;                // change of normalized position per unit a
-    float a0;                        // first sample on the grid a0 + i * step
-    int n;                           // samples inside the volume
+    float px, py, pz;                    // normalized position at a = 0
+    float dx, dy, dz;                    // change of normalized position per unit a
+    float a0;                            // first sample on the grid a0 + i * step
+    int n;                               // samples inside the volume
 };
 
-__device__ __forceinline__ Ray make_ray(const DvrParams &P, int x, int y) {
+__device__ __forceinline__ Ray make_ray(const DvrBatch &B, const DvrView &V, int x, int y) {
     Ray r;
-    const float u = (x - P.W / 2.0f - P.xT) / P.H;
-    const float v = (y - P.H / 2.0f - P.yT) / P.H;
+    const float u = (x - B.W / 2.0f - V.xT) / B.H;
+    const float v = (y - B.H / 2.0f - V.yT) / B.H;
     float base[3], dir[3];
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
         // pos(a) = M (u, (a - 0.866) s, v) * mls + 0.5
-        base[k] = (P.M[3 * k] * u + P.M[3 * k + 1] * (-0.866f * P.scale) + P.M[3 * k + 2] * v) * P.mls[k] + 0.5f;
-        dir[k] = P.M[3 * k + 1] * P.scale * P.mls[k];
+        base[k] = (V.M[3 * k] * u + V.M[3 * k + 1] * (-0.866f * V.scale) + V.M[3 * k + 2] * v) * V.mls[k] + 0.5f;
+        dir[k] = V.M[3 * k + 1] * V.scale * V.mls[k];
     }
     float lo = 0.0f, hi = 1.732f;
     bool hit = true;
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
         if (fabsf(dir[k]) < 1e-12f) {
             if (base[k] < 0.0f || base[k] > 1.0f) hit = false;
@@ -88,78 +102,106 @@ __device__ __forceinline__ Ray make_ray(const DvrParams &P, int x, int y) {
     r.dx = dir[0];
     r.dy = dir[1];
     r.dz = dir[2];
-    r.a0 = ceilf(lo / P.step) * P.step;
-    r.n = (hit && lo < hi) ? max(0, (int)floorf((hi - r.a0) / P.step) + 1) : 0;
+    r.a0 = ceilf(lo / V.step) * V.step;
+    r.n = (hit && lo < hi) ? max(0, (int)floorf((hi - r.a0) / V.step) + 1) : 0;
     return r;
 }
 
-struct Sample {
-    int i0[3];
-    float w[3];
-    float s;
+// Cell and weights of sample i: texel coordinate pos*dim - 0.5, its integer
+// part and fraction.  One expression (explicit fused multiply-adds) serves the
+// forward and backward kernels, so both see the same cells and weights.
+struct Cell {
+    int ix, iy, iz;
+    float wx, wy, wz;
 };
 
-__device__ __forceinline__ void trilinear(const DvrParams &P, const float *__restrict__ vol, const Ray &r, int i,
-                                          Sample &S) {
-    const float a = r.a0 + i * P.step;
-    const float c[3] = {(r.px + a * r.dx) * P.fdim[0] - 0.5f, (r.py + a * r.dy) * P.fdim[1] - 0.5f,
-                        (r.pz + a * r.dz) * P.fdim[2] - 0.5f};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float f = floorf(c[k]);
-        S.i0[k] = (int)f;
-        S.w[k] = c[k] - f;
-    }
-    float acc = 0.0f;
-#pragma unroll
-    for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-            for (int dx = 0; dx < 2; ++dx) {
-                const int ix = min(max(S.i0[0] + dx, 0), P.dim[0] - 1);
-                const int iy = min(max(S.i0[1] + dy, 0), P.dim[1] - 1);
-                const int iz = min(max(S.i0[2] + dz, 0), P.dim[2] - 1);
-                const float wt = (dx ? S.w[0] : 1.0f - S.w[0]) * (dy ? S.w[1] : 1.0f - S.w[1]) *
-                                 (dz ? S.w[2] : 1.0f - S.w[2]);
-                acc += wt * __ldg(&vol[((size_t)iz * P.dim[1] + iy) * P.dim[0] + ix]);
-            }
-    S.s = acc;
+__device__ __forceinline__ Cell sample_cell(const DvrBatch &B, const Ray &r, float step, int i) {
+    const float a = __fmaf_rn((float)i, step, r.a0);
+    const float cx = __fmaf_rn(__fmaf_rn(a, r.dx, r.px), B.fdim[0], -0.5f);
+    const float cy = __fmaf_rn(__fmaf_rn(a, r.dy, r.py), B.fdim[1], -0.5f);
+    const float cz = __fmaf_rn(__fmaf_rn(a, r.dz, r.pz), B.fdim[2], -0.5f);
+    const float fx = floorf(cx), fy = floorf(cy), fz = floorf(cz);
+    Cell c;
+    c.ix = (int)fx;
+    c.iy = (int)fy;
+    c.iz = (int)fz;
+    c.wx = cx - fx;
+    c.wy = cy - fy;
+    c.wz = cz - fz;
+    return c;
 }
 
-struct LutHit {
-    int k0, k1;
-    float w;                         // weight of k1
-    float slope;                     // d(LUT coordinate)/d(value): n inside, 0 where clamped
-};
+__device__ __forceinline__ float lerp(float a, float b, float w) { return __fmaf_rn(w, b - a, a); }
 
-__device__ __forceinline__ LutHit lut_index(const DvrParams &P, float s) {
-    LutHit h;
-    const int n = P.lut_len;
-    const float x = s * n - 0.5f;
-    const float f = floorf(x);
-    const int k = (int)f;
-    if (k < 0) {
-        h.k0 = h.k1 = 0;
-        h.w = 0.0f;
-        h.slope = 0.0f;
-    } else if (k >= n - 1) {
-        h.k0 = h.k1 = n - 1;
-        h.w = 0.0f;
-        h.slope = 0.0f;
+// Trilinear value of a cell; cells inside the volume read their eight voxels
+// without clamping (the common case), the boundary half-voxel clamps to edge.
+__device__ __forceinline__ float trilinear(const DvrBatch &B, const float *__restrict__ vol, const Cell &c) {
+    const int X = B.dim[0];
+    float v0, v1, v2, v3, v4, v5, v6, v7;
+    if ((unsigned)c.ix < (unsigned)(X - 1) && (unsigned)c.iy < (unsigned)(B.dim[1] - 1) &&
+        (unsigned)c.iz < (unsigned)(B.dim[2] - 1)) {
+        const float *p = vol + (c.iz * B.sxy + c.iy * X + c.ix);
+        v0 = __ldg(p);
+        v1 = __ldg(p + 1);
+        v2 = __ldg(p + X);
+        v3 = __ldg(p + X + 1);
+        p += B.sxy;
+        v4 = __ldg(p);
+        v5 = __ldg(p + 1);
+        v6 = __ldg(p + X);
+        v7 = __ldg(p + X + 1);
     } else {
-        h.k0 = k;
-        h.k1 = k + 1;
-        h.w = x - f;
-        h.slope = (float)n;
+        const int x0 = min(max(c.ix, 0), X - 1), x1 = min(max(c.ix + 1, 0), X - 1);
+        const int y0 = min(max(c.iy, 0), B.dim[1] - 1) * X, y1 = min(max(c.iy + 1, 0), B.dim[1] - 1) * X;
+        const int z0 = min(max(c.iz, 0), B.dim[2] - 1) * B.sxy, z1 = min(max(c.iz + 1, 0), B.dim[2] - 1) * B.sxy;
+        v0 = __ldg(vol + z0 + y0 + x0);
+        v1 = __ldg(vol + z0 + y0 + x1);
+        v2 = __ldg(vol + z0 + y1 + x0);
+        v3 = __ldg(vol + z0 + y1 + x1);
+        v4 = __ldg(vol + z1 + y0 + x0);
+        v5 = __ldg(vol + z1 + y0 + x1);
+        v6 = __ldg(vol + z1 + y1 + x0);
+        v7 = __ldg(vol + z1 + y1 + x1);
     }
-    return h;
+    const float a0 = lerp(v0, v1, c.wx), a1 = lerp(v2, v3, c.wx), a2 = lerp(v4, v5, c.wx), a3 = lerp(v6, v7, c.wx);
+    return lerp(lerp(a0, a1, c.wy), lerp(a2, a3, c.wy), c.wz);
 }
 
-__device__ __forceinline__ float4 lut_fetch(const float4 *lut, const LutHit &h) {
-    const float4 a = lut[h.k0], b = lut[h.k1];
-    return make_float4(a.x + h.w * (b.x - a.x), a.y + h.w * (b.y - a.y), a.z + h.w * (b.z - a.z),
-                       a.w + h.w * (b.w - a.w));
+// LUT lookup: x = s*n - 0.5 clamped to [0, n-1]; cell k = floor, weight w of
+// entry k+1.  L[k] holds the entries, D[k] = L[k+1] - L[k] (D[n-1] = 0).
+struct LutCell {
+    int k;
+    float w;
+    bool inside;                         // 0 <= x < n-1: the value's slope is n
+};
+
+__device__ __forceinline__ LutCell lut_cell(float s, int n) {
+    LutCell c;
+    const float x = __fmaf_rn(s, (float)n, -0.5f);
+    c.inside = (x >= 0.0f) && (x < (float)(n - 1));
+    const float xc = fminf(fmaxf(x, 0.0f), (float)(n - 1));
+    c.k = (int)xc;
+    c.w = xc - (float)c.k;
+    return c;
+}
+
+__device__ __forceinline__ float4 lut_value(const float4 *L, const float4 *D, const LutCell &c) {
+    const float4 a = L[c.k], d = D[c.k];
+    return make_float4(__fmaf_rn(c.w, d.x, a.x), __fmaf_rn(c.w, d.y, a.y), __fmaf_rn(c.w, d.z, a.z),
+                       __fmaf_rn(c.w, d.w, a.w));
+}
+
+__device__ __forceinline__ void load_lut(const float4 *__restrict__ lut_g, float4 *L, float4 *D, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float4 a = lut_g[i];
+        L[i] = a;
+        if (i + 1 < n) {
+            const float4 b = lut_g[i + 1];
+            D[i] = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, b.w - a.w);
+        } else {
+            D[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
 }
 
 __device__ __forceinline__ int pixel_x(int bx, int tile_w) {
@@ -173,255 +215,335 @@ __device__ __forceinline__ int pixel_y(int by, int tile_w) {
 }
 
 // ---------------------------------------------------------------------------
-// forward: 256 threads = 32x8 pixels as 8x4 warp tiles
+// forward: 256 threads = 32x8 pixels as 8x4 warp tiles; blockIdx.z = view
 
-__global__ void __launch_bounds__(256) k_dvr_forward(DvrParams P, const float *__restrict__ vol,
-                                                     const float4 *__restrict__ lut_g, float *__restrict__ image,
+__global__ void __launch_bounds__(256) k_dvr_forward(const __grid_constant__ DvrBatch B,
+                                                     const float *__restrict__ vol,
+                                                     const float4 *__restrict__ lut_g, float *__restrict__ images,
                                                      float *__restrict__ trans, float *__restrict__ work) {
-    __shared__ float4 lut[kDvrMaxLut];
-    for (int i = threadIdx.x; i < P.lut_len; i += blockDim.x) lut[i] = lut_g[i];
+    extern __shared__ float4 sm[];
+    float4 *L = sm, *D = sm + B.lut_len;
+    load_lut(lut_g, L, D, B.lut_len);
     __syncthreads();
+    const DvrView &V = B.v[blockIdx.z];
     const int x = pixel_x(blockIdx.x, 32), y = pixel_y(blockIdx.y, 32);
-    if (x >= P.W || y >= P.H) return;
-    const size_t pix = (size_t)y * P.W + x, npix = (size_t)P.W * P.H;
+    if (x >= B.W || y >= B.H) return;
+    const size_t npix = (size_t)B.W * B.H, pix = (size_t)y * B.W + x;
+    float *wk = work ? work + V.work_off : nullptr;
+    const int cmask = (1 << V.ckpt_shift) - 1;
     float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
-    const Ray r = make_ray(P, x, y);
+    const Ray r = make_ray(B, V, x, y);
     int i = 0;
     for (; i < r.n; ++i) {
-        if (work && (i % P.ckpt) == 0) work[(size_t)(i / P.ckpt) * npix + pix] = T;
-        Sample S;
-        trilinear(P, vol, r, i, S);
-        const float4 c = lut_fetch(lut, lut_index(P, S.s));
+        if (wk && (i & cmask) == 0) wk[(size_t)(i >> V.ckpt_shift) * npix + pix] = T;
+        const float s = trilinear(B, vol, sample_cell(B, r, V.step, i));
+        const float4 c = lut_value(L, D, lut_cell(s, B.lut_len));
         const float wgt = T * c.w;
-        cr += wgt * c.x;
-        cg += wgt * c.y;
-        cb += wgt * c.z;
+        cr = __fmaf_rn(wgt, c.x, cr);
+        cg = __fmaf_rn(wgt, c.y, cg);
+        cb = __fmaf_rn(wgt, c.z, cb);
         T *= (1.0f - c.w);
-        if (T < P.t_min) {
+        if (T < V.t_min) {
             ++i;
             break;
         }
     }
-    image[3 * pix + 0] = cr;
-    image[3 * pix + 1] = cg;
-    image[3 * pix + 2] = cb;
-    trans[pix] = T;
-    if (work) reinterpret_cast<int *>(work + (size_t)P.max_ckpt * npix)[pix] = i;   // samples taken
+    const size_t o = (size_t)blockIdx.z * npix + pix;
+    images[3 * o + 0] = cr;
+    images[3 * o + 1] = cg;
+    images[3 * o + 2] = cb;
+    trans[o] = T;
+    if (wk) reinterpret_cast<int *>(wk + (size_t)V.max_ckpt * npix)[pix] = i;   // samples taken
 }
 
 // ---------------------------------------------------------------------------
-// backward: 128 threads = 16x8 pixels as 8x4 warp tiles
+// backward: 128 threads = 16x8 pixels as 8x4 warp tiles; blockIdx.z = view
 
-__device__ __forceinline__ void bin_add(float *bins, int k, float4 v) {
-    // lanes that hit the same entry add their values first (warp shuffle),
-    // then one lane per entry updates the shared-memory bin
-    const unsigned active = __activemask();
-    const unsigned same = __match_any_sync(active, k);
-    const int leader = __ffs(same) - 1;
-    const int lane = threadIdx.x & 31;
-    float4 acc = v;
-    if (__popc(same) > 1) {
-        // sum over the lanes of `same` by walking their bits (groups are small)
-        acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (unsigned m = same; m; m &= m - 1) {
-            const int src = __ffs(m) - 1;
-            acc.x += __shfl_sync(same, v.x, src);
-            acc.y += __shfl_sync(same, v.y, src);
-            acc.z += __shfl_sync(same, v.z, src);
-            acc.w += __shfl_sync(same, v.w, src);
-        }
-    }
-    if (lane == leader) {
-        atomicAdd(&bins[4 * k + 0], acc.x);
-        atomicAdd(&bins[4 * k + 1], acc.y);
-        atomicAdd(&bins[4 * k + 2], acc.z);
-        atomicAdd(&bins[4 * k + 3], acc.w);
+__device__ __forceinline__ void flush_lut(float *bins, int n, int k, const float4 &a0, const float4 &a1) {
+    if (k < 0) return;
+    atomicAdd(&bins[4 * k + 0], a0.x);
+    atomicAdd(&bins[4 * k + 1], a0.y);
+    atomicAdd(&bins[4 * k + 2], a0.z);
+    atomicAdd(&bins[4 * k + 3], a0.w);
+    if (k + 1 < n) {
+        atomicAdd(&bins[4 * k + 4], a1.x);
+        atomicAdd(&bins[4 * k + 5], a1.y);
+        atomicAdd(&bins[4 * k + 6], a1.z);
+        atomicAdd(&bins[4 * k + 7], a1.w);
     }
 }
 
-__global__ void __launch_bounds__(128) k_dvr_backward(DvrParams P, const float *__restrict__ vol,
+__device__ __forceinline__ void flush_vol(float *__restrict__ gv, const DvrBatch &B, int ix, int iy, int iz,
+                                          const float (&acc)[8]) {
+    if (ix == INT_MIN) return;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        if (acc[c] == 0.0f) continue;
+        const int x = min(max(ix + (c & 1), 0), B.dim[0] - 1);
+        const int y = min(max(iy + ((c >> 1) & 1), 0), B.dim[1] - 1);
+        const int z = min(max(iz + (c >> 2), 0), B.dim[2] - 1);
+        atomicAdd(&gv[z * B.sxy + y * B.dim[0] + x], acc[c]);
+    }
+}
+
+template <bool VOLGRAD>
+__global__ void __launch_bounds__(128) k_dvr_backward(const __grid_constant__ DvrBatch B,
+                                                      const float *__restrict__ vol,
                                                       const float4 *__restrict__ lut_g,
                                                       const float *__restrict__ work,
-                                                      const float *__restrict__ grad_image,
+                                                      const float *__restrict__ grad_images,
                                                       float *__restrict__ grad_lut, float *__restrict__ grad_vol) {
-    __shared__ float4 lut[kDvrMaxLut];
-    __shared__ float bins[kDvrMaxLut * 4];
-    for (int i = threadIdx.x; i < P.lut_len; i += blockDim.x) {
-        lut[i] = lut_g[i];
-        bins[4 * i] = bins[4 * i + 1] = bins[4 * i + 2] = bins[4 * i + 3] = 0.0f;
-    }
+    extern __shared__ float4 sm[];
+    const int n = B.lut_len;
+    float4 *L = sm, *D = sm + n;
+    float *bins = reinterpret_cast<float *>(sm + 2 * n);
+    load_lut(lut_g, L, D, n);
+    for (int i = threadIdx.x; i < 4 * n; i += blockDim.x) bins[i] = 0.0f;
     __syncthreads();
+
+    const DvrView &V = B.v[blockIdx.z];
     const int x = pixel_x(blockIdx.x, 16), y = pixel_y(blockIdx.y, 16);
-    const size_t npix = (size_t)P.W * P.H;
-    int n = 0;
-    float gr = 0.f, gg = 0.f, gb = 0.f;
-    Ray r;
-    size_t pix = 0;
-    if (x < P.W && y < P.H) {
-        pix = (size_t)y * P.W + x;
-        n = reinterpret_cast<const int *>(work + (size_t)P.max_ckpt * npix)[pix];
-        gr = grad_image[3 * pix];
-        gg = grad_image[3 * pix + 1];
-        gb = grad_image[3 * pix + 2];
-        if (gr == 0.0f && gg == 0.0f && gb == 0.0f) n = 0;
-        r = make_ray(P, x, y);
-    }
-    // lanes with nothing to do still take part in the warp-wide bin updates
-    float Ur = 0.f, Ug = 0.f, Ub = 0.f;
-    const int nseg = (n + kDvrSeg - 1) / kDvrSeg;
-    const int wseg = __reduce_max_sync(0xffffffffu, nseg);
-    for (int seg = wseg - 1; seg >= 0; --seg) {
-        const bool live = seg < nseg;
-        float Ts[kDvrSeg];
-        int s1 = 0;
-        if (live) {
+    if (x < B.W && y < B.H) {
+        const size_t npix = (size_t)B.W * B.H, pix = (size_t)y * B.W + x;
+        const float *wk = work + V.work_off;
+        const size_t o = (size_t)blockIdx.z * npix + pix;
+        const float gr = grad_images[3 * o], gg = grad_images[3 * o + 1], gb = grad_images[3 * o + 2];
+        int ns = reinterpret_cast<const int *>(wk + (size_t)V.max_ckpt * npix)[pix];
+        if (gr == 0.0f && gg == 0.0f && gb == 0.0f) ns = 0;
+        const Ray r = make_ray(B, V, x, y);
+        float Ur = 0.f, Ug = 0.f, Ub = 0.f;
+        int lk = -1;
+        float4 la0 = make_float4(0.f, 0.f, 0.f, 0.f), la1 = la0;
+        int vx = INT_MIN, vy = 0, vz = 0;
+        float va[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) va[c] = 0.0f;
+
+        for (int seg = (ns + kDvrSeg - 1) / kDvrSeg - 1; seg >= 0; --seg) {
             const int s0 = seg * kDvrSeg;
-            const int c = s0 / P.ckpt;
-            float T = work[(size_t)c * npix + pix];
-            for (int i = c * P.ckpt; i < s0; ++i) {
-                Sample S;
-                trilinear(P, vol, r, i, S);
-                T *= 1.0f - lut_fetch(lut, lut_index(P, S.s)).w;
-            }
-            s1 = min(s0 + kDvrSeg, n) - s0;
+            const int c0 = s0 >> V.ckpt_shift;
+            float T = wk[(size_t)c0 * npix + pix];
+            for (int i = c0 << V.ckpt_shift; i < s0; ++i)
+                T *= 1.0f - lut_value(L, D, lut_cell(trilinear(B, vol, sample_cell(B, r, V.step, i)), n)).w;
+            const int s1 = min(s0 + kDvrSeg, ns) - s0;
+            float Ts[kDvrSeg], Ss[kDvrSeg];
 #pragma unroll
             for (int j = 0; j < kDvrSeg; ++j) {
                 Ts[j] = T;
+                Ss[j] = 0.0f;
                 if (j < s1) {
-                    Sample S;
-                    trilinear(P, vol, r, s0 + j, S);
-                    T *= 1.0f - lut_fetch(lut, lut_index(P, S.s)).w;
+                    const float s = trilinear(B, vol, sample_cell(B, r, V.step, s0 + j));
+                    Ss[j] = s;
+                    T *= 1.0f - lut_value(L, D, lut_cell(s, n)).w;
                 }
             }
-        }
 #pragma unroll
-        for (int j = kDvrSeg - 1; j >= 0; --j) {
-            const bool on = live && j < s1;
-            LutHit h;
-            h.k0 = h.k1 = 0;
-            h.w = 0.f;
-            h.slope = 0.f;
-            float4 d0 = make_float4(0.f, 0.f, 0.f, 0.f), d1 = d0;
-            Sample S;
-            float d_cr = 0.f, d_cg = 0.f, d_cb = 0.f, d_a = 0.f;
-            if (on) {
-                trilinear(P, vol, r, seg * kDvrSeg + j, S);
-                h = lut_index(P, S.s);
-                const float4 q = lut_fetch(lut, h);
+            for (int j = kDvrSeg - 1; j >= 0; --j) {
+                if (j >= s1) continue;
+                const LutCell h = lut_cell(Ss[j], n);
+                const float4 q = lut_value(L, D, h);
                 const float Ti = Ts[j];
-                d_cr = Ti * q.w * gr;
-                d_cg = Ti * q.w * gg;
-                d_cb = Ti * q.w * gb;
-                d_a = Ti * (gr * (q.x - Ur) + gg * (q.y - Ug) + gb * (q.z - Ub));
+                const float d_cr = Ti * q.w * gr, d_cg = Ti * q.w * gg, d_cb = Ti * q.w * gb;
+                const float d_a = Ti * (gr * (q.x - Ur) + gg * (q.y - Ug) + gb * (q.z - Ub));
                 Ur = q.w * q.x + (1.0f - q.w) * Ur;
                 Ug = q.w * q.y + (1.0f - q.w) * Ug;
                 Ub = q.w * q.z + (1.0f - q.w) * Ub;
+                if (h.k != lk) {
+                    flush_lut(bins, n, lk, la0, la1);
+                    lk = h.k;
+                    la0 = make_float4(0.f, 0.f, 0.f, 0.f);
+                    la1 = la0;
+                }
                 const float w1 = h.w, w0 = 1.0f - h.w;
-                d0 = make_float4(w0 * d_cr, w0 * d_cg, w0 * d_cb, w0 * d_a);
-                d1 = make_float4(w1 * d_cr, w1 * d_cg, w1 * d_cb, w1 * d_a);
-            }
-            bin_add(bins, h.k0, d0);
-            bin_add(bins, h.k1, d1);
-            if (on && grad_vol && h.slope != 0.0f) {
-                const float4 L0 = lut[h.k0], L1 = lut[h.k1];
-                const float ds = h.slope * (d_cr * (L1.x - L0.x) + d_cg * (L1.y - L0.y) + d_cb * (L1.z - L0.z) +
-                                            d_a * (L1.w - L0.w));
-                if (ds != 0.0f) {
+                la0.x += w0 * d_cr;
+                la0.y += w0 * d_cg;
+                la0.z += w0 * d_cb;
+                la0.w += w0 * d_a;
+                la1.x += w1 * d_cr;
+                la1.y += w1 * d_cg;
+                la1.z += w1 * d_cb;
+                la1.w += w1 * d_a;
+                if (VOLGRAD && h.inside) {
+                    const float4 d = D[h.k];
+                    const float ds = (float)n * (d_cr * d.x + d_cg * d.y + d_cb * d.z + d_a * d.w);
+                    if (ds != 0.0f) {
+                        const Cell c = sample_cell(B, r, V.step, s0 + j);
+                        if (c.ix != vx || c.iy != vy || c.iz != vz) {
+                            flush_vol(grad_vol, B, vx, vy, vz, va);
+                            vx = c.ix;
+                            vy = c.iy;
+                            vz = c.iz;
 #pragma unroll
-                    for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-                        for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-                            for (int dx = 0; dx < 2; ++dx) {
-                                const int ix = min(max(S.i0[0] + dx, 0), P.dim[0] - 1);
-                                const int iy = min(max(S.i0[1] + dy, 0), P.dim[1] - 1);
-                                const int iz = min(max(S.i0[2] + dz, 0), P.dim[2] - 1);
-                                const float wt = (dx ? S.w[0] : 1.0f - S.w[0]) * (dy ? S.w[1] : 1.0f - S.w[1]) *
-                                                 (dz ? S.w[2] : 1.0f - S.w[2]);
-                                atomicAdd(&grad_vol[((size_t)iz * P.dim[1] + iy) * P.dim[0] + ix], wt * ds);
-                            }
+                            for (int k = 0; k < 8; ++k) va[k] = 0.0f;
+                        }
+                        const float y0z0 = (1.0f - c.wy) * (1.0f - c.wz) * ds, y1z0 = c.wy * (1.0f - c.wz) * ds;
+                        const float y0z1 = (1.0f - c.wy) * c.wz * ds, y1z1 = c.wy * c.wz * ds;
+                        va[0] += (1.0f - c.wx) * y0z0;
+                        va[1] += c.wx * y0z0;
+                        va[2] += (1.0f - c.wx) * y1z0;
+                        va[3] += c.wx * y1z0;
+                        va[4] += (1.0f - c.wx) * y0z1;
+                        va[5] += c.wx * y0z1;
+                        va[6] += (1.0f - c.wx) * y1z1;
+                        va[7] += c.wx * y1z1;
+                    }
                 }
             }
         }
+        flush_lut(bins, n, lk, la0, la1);
+        if (VOLGRAD) flush_vol(grad_vol, B, vx, vy, vz, va);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < P.lut_len * 4; i += blockDim.x) {
+    for (int i = threadIdx.x; i < 4 * n; i += blockDim.x) {
         const float v = bins[i];
         if (v != 0.0f) atomicAdd(&grad_lut[i], v);
     }
 }
 
-static int fill(const mk_dvr_params *p, DvrParams &P) {
-    if (!p || p->width <= 0 || p->height <= 0 || p->width > 16384 || p->height > 16384 || p->dims[0] <= 0 ||
-        p->dims[1] <= 0 || p->dims[2] <= 0 || p->lut_len < 2 || p->lut_len > kDvrMaxLut || !(p->step > 0.0f) ||
-        !(p->scale > 0.0f) || p->step < 1e-5f) {
-        set_last_error("mk_dvr: bad parameters (image size, dims, 2 <= lut_len <= 1024, 1e-5 <= step, scale > 0)");
+// ---------------------------------------------------------------------------
+// host side
+
+// Checkpoint spacing of a view: 16 samples, doubled until at most 512
+// checkpoints cover the longest ray (1.732 in the ray parameter).
+static void view_layout(const mk_dvr_params &p, int &ckpt_shift, int &max_ckpt) {
+    const int steps = (int)(1.74f / p.step) + 2;
+    int sh = 4;
+    while (((steps + (1 << sh) - 1) >> sh) > kDvrMaxCkpt) ++sh;
+    ckpt_shift = sh;
+    max_ckpt = (steps + (1 << sh) - 1) >> sh;
+}
+
+// Workspace floats of one view: max_ckpt checkpoint planes + one plane of counts.
+static size_t view_floats(const mk_dvr_params &p) {
+    int sh, mc;
+    view_layout(p, sh, mc);
+    return (size_t)(mc + 1) * p.width * p.height;
+}
+
+static int check_views(const mk_dvr_params *views, int nviews) {
+    if (!views || nviews <= 0) {
+        set_last_error("mk_dvr: no views");
         return MK_ERR_INVALID_ARGUMENT;
     }
-    P.W = p->width;
-    P.H = p->height;
-    for (int k = 0; k < 3; ++k) {
-        P.dim[k] = p->dims[k];
-        P.fdim[k] = (float)p->dims[k];
-        P.mls[k] = p->max_len_spacing[k];
+    const mk_dvr_params &a = views[0];
+    for (int i = 0; i < nviews; ++i) {
+        const mk_dvr_params &p = views[i];
+        if (p.width <= 0 || p.height <= 0 || p.width > 16384 || p.height > 16384 || p.dims[0] <= 0 ||
+            p.dims[1] <= 0 || p.dims[2] <= 0 || p.lut_len < 2 || p.lut_len > kDvrMaxLut || !(p.step >= 1e-5f) ||
+            !(p.scale > 0.0f) || !(p.t_min >= 0.0f)) {
+            set_last_error("mk_dvr: bad view parameters (image size 1..16384, dims > 0, 2 <= lut_len <= 1024, "
+                           "step >= 1e-5, scale > 0, t_min >= 0)");
+            return MK_ERR_INVALID_ARGUMENT;
+        }
+        if ((double)p.dims[0] * p.dims[1] * p.dims[2] >= 2147483648.0) {
+            set_last_error("mk_dvr: the volume must have fewer than 2^31 voxels");
+            return MK_ERR_INVALID_ARGUMENT;
+        }
+        if (p.width != a.width || p.height != a.height || p.lut_len != a.lut_len || p.dims[0] != a.dims[0] ||
+            p.dims[1] != a.dims[1] || p.dims[2] != a.dims[2]) {
+            set_last_error("mk_dvr: the views of one call must share width, height, dims and lut_len");
+            return MK_ERR_INVALID_ARGUMENT;
+        }
     }
-    for (int i = 0; i < 9; ++i) P.M[i] = p->transform[i];
-    P.scale = p->scale;
-    P.xT = p->x_translate;
-    P.yT = p->y_translate;
-    P.step = p->step;
-    P.t_min = p->t_min;
-    P.lut_len = p->lut_len;
-    const int steps = (int)(1.74f / p->step) + 2;
-    int ck = kDvrSeg;
-    while ((steps + ck - 1) / ck > kDvrMaxCkpt) ck *= 2;
-    P.ckpt = ck;
-    P.max_ckpt = (steps + ck - 1) / ck;
     return MK_OK;
+}
+
+static void fill_batch(const mk_dvr_params *views, int first, int count, size_t work_off0, DvrBatch &B) {
+    memset(&B, 0, sizeof(B));
+    const mk_dvr_params &a = views[first];
+    B.W = a.width;
+    B.H = a.height;
+    B.lut_len = a.lut_len;
+    for (int k = 0; k < 3; ++k) {
+        B.dim[k] = a.dims[k];
+        B.fdim[k] = (float)a.dims[k];
+    }
+    B.sxy = a.dims[0] * a.dims[1];
+    size_t off = work_off0;
+    for (int i = 0; i < count; ++i) {
+        const mk_dvr_params &p = views[first + i];
+        DvrView &V = B.v[i];
+        for (int m = 0; m < 9; ++m) V.M[m] = p.transform[m];
+        for (int k = 0; k < 3; ++k) V.mls[k] = p.max_len_spacing[k];
+        V.scale = p.scale;
+        V.xT = p.x_translate;
+        V.yT = p.y_translate;
+        V.step = p.step;
+        V.t_min = p.t_min;
+        view_layout(p, V.ckpt_shift, V.max_ckpt);
+        V.work_off = off;
+        off += view_floats(p);
+    }
 }
 
 }  // namespace mk
 
 using namespace mk;
 
-extern "C" int mk_dvr_workspace_floats(const mk_dvr_params *params, size_t *floats) {
-    DvrParams P;
-    if (!floats) return MK_ERR_INVALID_ARGUMENT;
-    int rc = fill(params, P);
-    if (rc != MK_OK) return rc;
-    *floats = (size_t)(P.max_ckpt + 1) * P.W * P.H;
-    return MK_OK;
-}
-
-extern "C" int mk_dvr_forward(const mk_dvr_params *params, const float *volume, const float *lut, float *image,
-                              float *transmittance, float *workspace, void *stream) {
-    DvrParams P;
-    int rc = fill(params, P);
-    if (rc != MK_OK) return rc;
-    if (!volume || !lut || !image || !transmittance) {
-        set_last_error("mk_dvr_forward: null pointer");
+extern "C" int mk_dvr_workspace_floats(const mk_dvr_params *views, int nviews, size_t *floats) {
+    if (!floats) {
+        set_last_error("mk_dvr_workspace_floats: null argument");
         return MK_ERR_INVALID_ARGUMENT;
     }
-    dim3 grid((P.W + 31) / 32, (P.H + 7) / 8);
-    k_dvr_forward<<<grid, 256, 0, (cudaStream_t)stream>>>(P, volume, reinterpret_cast<const float4 *>(lut), image,
-                                                         transmittance, workspace);
-    MK_CUDA_TRY(cudaGetLastError());
+    int rc = check_views(views, nviews);
+    if (rc != MK_OK) return rc;
+    size_t total = 0;
+    for (int i = 0; i < nviews; ++i) total += view_floats(views[i]);
+    *floats = total;
     return MK_OK;
 }
 
-extern "C" int mk_dvr_backward(const mk_dvr_params *params, const float *volume, const float *lut,
-                               const float *workspace, const float *grad_image, float *grad_lut,
+extern "C" int mk_dvr_forward(const mk_dvr_params *views, int nviews, const float *volume, const float *lut,
+                              float *images, float *transmittance, float *workspace, void *stream) {
+    if (!volume || !lut || !images || !transmittance) {
+        set_last_error("mk_dvr_forward: null argument");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    int rc = check_views(views, nviews);
+    if (rc != MK_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t npix = (size_t)views[0].width * views[0].height;
+    const size_t smem = 2 * (size_t)views[0].lut_len * sizeof(float4);
+    MK_CUDA_TRY(cudaFuncSetAttribute(k_dvr_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    size_t off = 0;
+    DvrBatch B;
+    for (int first = 0; first < nviews; first += kDvrViewsPerLaunch) {
+        const int count = min(kDvrViewsPerLaunch, nviews - first);
+        fill_batch(views, first, count, off, B);
+        for (int i = 0; i < count; ++i) off += view_floats(views[first + i]);
+        dim3 grid((B.W + 31) / 32, (B.H + 7) / 8, count);
+        k_dvr_forward<<<grid, 256, smem, s>>>(B, volume, reinterpret_cast<const float4 *>(lut),
+                                              images + (size_t)first * npix * 3, transmittance + (size_t)first * npix,
+                                              workspace);
+        MK_CUDA_TRY(cudaGetLastError());
+    }
+    return MK_OK;
+}
+
+extern "C" int mk_dvr_backward(const mk_dvr_params *views, int nviews, const float *volume, const float *lut,
+                               const float *workspace, const float *grad_images, float *grad_lut,
                                float *grad_volume, void *stream) {
-    DvrParams P;
-    int rc = fill(params, P);
-    if (rc != MK_OK) return rc;
-    if (!volume || !lut || !workspace || !grad_image || !grad_lut) {
-        set_last_error("mk_dvr_backward: null pointer");
+    if (!volume || !lut || !workspace || !grad_images || !grad_lut) {
+        set_last_error("mk_dvr_backward: null argument");
         return MK_ERR_INVALID_ARGUMENT;
     }
-    dim3 grid((P.W + 15) / 16, (P.H + 7) / 8);
-    k_dvr_backward<<<grid, 128, 0, (cudaStream_t)stream>>>(P, volume, reinterpret_cast<const float4 *>(lut), workspace,
-                                                          grad_image, grad_lut, grad_volume);
-    MK_CUDA_TRY(cudaGetLastError());
+    int rc = check_views(views, nviews);
+    if (rc != MK_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t npix = (size_t)views[0].width * views[0].height;
+    const size_t smem = 3 * (size_t)views[0].lut_len * sizeof(float4);
+    auto kern = grad_volume ? k_dvr_backward<true> : k_dvr_backward<false>;
+    MK_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    size_t off = 0;
+    DvrBatch B;
+    for (int first = 0; first < nviews; first += kDvrViewsPerLaunch) {
+        const int count = min(kDvrViewsPerLaunch, nviews - first);
+        fill_batch(views, first, count, off, B);
+        for (int i = 0; i < count; ++i) off += view_floats(views[first + i]);
+        dim3 grid((B.W + 15) / 16, (B.H + 7) / 8, count);
+        kern<<<grid, 128, smem, s>>>(B, volume, reinterpret_cast<const float4 *>(lut), workspace,
+                                     grad_images + (size_t)first * npix * 3, grad_lut, grad_volume);
+        MK_CUDA_TRY(cudaGetLastError());
+    }
     return MK_OK;
 }

@@ -18,33 +18,12 @@ from __future__ import annotations
 import ctypes as C
 
 from . import capi
+from .capi import DVRParams
 from .camera import volume_factors
 
 
-class DVRParams(C.Structure):
-    _fields_ = [
-        ("width", C.c_int), ("height", C.c_int), ("dims", C.c_int * 3),
-        ("max_len_spacing", C.c_float * 3), ("transform", C.c_float * 9),
-        ("scale", C.c_float), ("x_translate", C.c_float), ("y_translate", C.c_float),
-        ("step", C.c_float), ("t_min", C.c_float), ("lut_len", C.c_int),
-    ]
-
-
-_bound = False
-
-
 def _lib():
-    global _bound
-    L = capi.lib()
-    if not _bound:
-        vp = C.c_void_p
-        L.mk_dvr_workspace_floats.argtypes = [C.POINTER(DVRParams), C.POINTER(C.c_size_t)]
-        L.mk_dvr_forward.argtypes = [C.POINTER(DVRParams), vp, vp, vp, vp, vp, vp]
-        L.mk_dvr_backward.argtypes = [C.POINTER(DVRParams), vp, vp, vp, vp, vp, vp, vp]
-        for f in ("mk_dvr_workspace_floats", "mk_dvr_forward", "mk_dvr_backward"):
-            getattr(L, f).restype = C.c_int
-        _bound = True
-    return L
+    return capi.lib()
 
 
 def dvr_params(width, height, camera, dims, spacing, step_voxels=0.5, t_min=1e-4, lut_len=256) -> DVRParams:
@@ -83,6 +62,19 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
+def view_array(views):
+    """The views as a C array of DVRParams (ctypes)."""
+    views = list(views)
+    return (DVRParams * len(views))(*views), len(views)
+
+
+def workspace_floats(views) -> int:
+    arr, n = view_array(views)
+    out = C.c_size_t(0)
+    _check(_lib().mk_dvr_workspace_floats(arr, n, C.byref(out)), "mk_dvr_workspace_floats")
+    return out.value
+
+
 def _torch_function():
     import torch
 
@@ -94,39 +86,36 @@ def _torch_function():
             volume = volume.detach().contiguous().float()
             lut = lut.detach().contiguous().float()
             L = _lib()
-            stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-            images, works = [], []
-            need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1]
-            for p in views:
+            arr, nv = view_array(views)
+            p0 = arr[0]
+            for p in arr:
                 if p.lut_len != lut.shape[0] or tuple(p.dims) != tuple(volume.shape[::-1]):
                     raise ValueError("view parameters do not match the volume or LUT")
-                img = torch.empty((p.height, p.width, 3), dtype=torch.float32, device=volume.device)
-                trans = torch.empty((p.height, p.width), dtype=torch.float32, device=volume.device)
-                work = None
-                if need:
-                    n = C.c_size_t(0)
-                    _check(L.mk_dvr_workspace_floats(C.byref(p), C.byref(n)), "mk_dvr_workspace_floats")
-                    work = torch.empty(n.value, dtype=torch.float32, device=volume.device)
-                _check(L.mk_dvr_forward(C.byref(p), _ptr(volume), _ptr(lut), _ptr(img), _ptr(trans), _ptr(work),
-                                        stream), "mk_dvr_forward")
-                images.append(img)
-                works.append(work)
-            ctx.views = views
-            ctx.works = works
+                if (p.width, p.height) != (p0.width, p0.height):
+                    raise ValueError("the views of one render must share width and height")
+            stream = C.c_void_p(torch.cuda.current_stream(volume.device).cuda_stream)
+            images = torch.empty((nv, p0.height, p0.width, 3), dtype=torch.float32, device=volume.device)
+            trans = torch.empty((nv, p0.height, p0.width), dtype=torch.float32, device=volume.device)
+            work = None
+            if ctx.needs_input_grad[0] or ctx.needs_input_grad[1]:
+                work = torch.empty(workspace_floats(arr), dtype=torch.float32, device=volume.device)
+            _check(L.mk_dvr_forward(arr, nv, _ptr(volume), _ptr(lut), _ptr(images), _ptr(trans), _ptr(work),
+                                    stream), "mk_dvr_forward")
+            ctx.views = arr
+            ctx.work = work
             ctx.save_for_backward(volume, lut)
-            return torch.stack(images)
+            return images
 
         @staticmethod
         def backward(ctx, grad_images):
             volume, lut = ctx.saved_tensors
             L = _lib()
-            stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            stream = C.c_void_p(torch.cuda.current_stream(volume.device).cuda_stream)
             grad_lut = torch.zeros_like(lut)
             grad_vol = torch.zeros_like(volume) if ctx.needs_input_grad[0] else None
             g = grad_images.contiguous().float()
-            for i, p in enumerate(ctx.views):
-                _check(L.mk_dvr_backward(C.byref(p), _ptr(volume), _ptr(lut), _ptr(ctx.works[i]), _ptr(g[i]),
-                                         _ptr(grad_lut), _ptr(grad_vol), stream), "mk_dvr_backward")
+            _check(L.mk_dvr_backward(ctx.views, len(ctx.views), _ptr(volume), _ptr(lut), _ptr(ctx.work), _ptr(g),
+                                     _ptr(grad_lut), _ptr(grad_vol), stream), "mk_dvr_backward")
             return grad_vol, (grad_lut if ctx.needs_input_grad[1] else None), None
 
     return VolumeRender

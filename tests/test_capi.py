@@ -79,3 +79,34 @@ def test_no_device_is_a_status_not_an_exit():
     with pytest.raises(capi.MonkeyGLError) as ei:
         capi.Volume(np.zeros((4, 4, 4), np.int16))
     assert ei.value.status == 7
+
+
+def test_dvr_host_validation():
+    """mk_dvr_* check their views on the host, before any launch."""
+    from monkeygl_b200 import dvr
+    from monkeygl_b200.camera import view_camera
+    a = dvr.dvr_params(64, 48, view_camera(0.0), (32, 32, 32), (1, 1, 1), 0.5, 0.0, 256)
+    b = dvr.dvr_params(64, 48, view_camera(30.0), (32, 32, 32), (1, 1, 1), 0.25, 0.0, 256)
+    # checkpoint planes (16 samples apart, 1.74/step + 2 samples) + one plane of counts
+    per = lambda p: (((int(1.74 / p.step) + 2 + 15) // 16) + 1) * 64 * 48
+    assert dvr.workspace_floats([a]) == per(a)
+    assert dvr.workspace_floats([a, b]) == per(a) + per(b)
+    L = dvr._lib()
+    n = C.c_size_t(0)
+    c = dvr.dvr_params(32, 48, view_camera(0.0), (32, 32, 32), (1, 1, 1))
+    for bad in ([a, c],):                                        # differing widths
+        arr, nv = dvr.view_array(bad)
+        assert L.mk_dvr_workspace_floats(arr, nv, C.byref(n)) == capi.MK_ERR_INVALID_ARGUMENT
+    for field, value in (("lut_len", 1), ("lut_len", 2000), ("step", 0.0), ("scale", 0.0), ("width", 0)):
+        p = dvr.dvr_params(64, 48, view_camera(0.0), (32, 32, 32), (1, 1, 1))
+        setattr(p, field, value)
+        arr, nv = dvr.view_array([p])
+        assert L.mk_dvr_workspace_floats(arr, nv, C.byref(n)) == capi.MK_ERR_INVALID_ARGUMENT
+        assert L.mk_dvr_forward(arr, nv, C.c_void_p(16), C.c_void_p(16), C.c_void_p(16), C.c_void_p(16),
+                                None, None) == capi.MK_ERR_INVALID_ARGUMENT
+    arr, nv = dvr.view_array([a])
+    assert L.mk_dvr_workspace_floats(arr, 0, C.byref(n)) == capi.MK_ERR_INVALID_ARGUMENT
+    assert L.mk_dvr_forward(arr, nv, None, C.c_void_p(16), C.c_void_p(16), C.c_void_p(16), None,
+                            None) == capi.MK_ERR_INVALID_ARGUMENT
+    assert L.mk_dvr_backward(arr, nv, C.c_void_p(16), C.c_void_p(16), None, C.c_void_p(16), C.c_void_p(16),
+                             None, None) == capi.MK_ERR_INVALID_ARGUMENT

@@ -183,34 +183,76 @@ def torch_reference(vol, lut, p, counts):
     return (T[..., None] * alpha[..., None] * q[..., :3]).sum(-2)
 
 
-def test_gradients_match_torch_autograd(setup):
-    vol, lut, target_lut, views = setup
-    target = torch.rand((64, 64, 3), device="cuda")
-    for p in views:
-        v = torch.tensor(vol, device="cuda", requires_grad=True)
-        l = torch.tensor(lut, device="cuda", requires_grad=True)
-        img = dvr.render(v, l, [p])[0]
-        ((img - target) ** 2).sum().backward()
-        # sample counts per ray from the kernel's workspace
-        L = dvr._lib()
-        nws = C.c_size_t(0)
-        L.mk_dvr_workspace_floats(C.byref(p), C.byref(nws))
-        work = torch.empty(nws.value, dtype=torch.float32, device="cuda")
-        img2 = torch.empty((64, 64, 3), device="cuda")
-        tr = torch.empty((64, 64), device="cuda")
-        L.mk_dvr_forward(C.byref(p), C.c_void_p(v.data_ptr()), C.c_void_p(l.data_ptr()), C.c_void_p(img2.data_ptr()),
-                         C.c_void_p(tr.data_ptr()), C.c_void_p(work.data_ptr()), None)
-        torch.cuda.synchronize()
-        counts = work[-64 * 64:].view(torch.int32).view(64, 64)
-        v2 = torch.tensor(vol, device="cuda", requires_grad=True)
-        l2 = torch.tensor(lut, device="cuda", requires_grad=True)
-        ref = torch_reference(v2, l2, p, counts)
-        ((ref - target) ** 2).sum().backward()
-        assert (img - ref).abs().max().item() < 1e-4
-        for name, a, b in (("lut", l.grad, l2.grad), ("volume", v.grad, v2.grad)):
-            rel = ((a - b).norm() / b.norm()).item()
-            print(f"{name}: relative error vs torch autograd {rel:.2e}")
-            assert rel < 1e-3
+@pytest.mark.parametrize("angle,t_min", [(0.0, 0.0), (50.0, 0.0), (30.0, 0.05)])
+def test_gradients_match_torch_autograd(setup, angle, t_min):
+    """Against autograd over the materialised samples; t_min > 0 stops rays
+    early, and the backward must stop them at the same sample."""
+    vol, lut, _, _ = setup
+    p = dvr.dvr_params(64, 64, view_camera(angle), (64, 64, 64), (1, 1, 1), 0.5, t_min, 256)
+    target = torch.rand((64, 64, 3), device="cuda", generator=torch.Generator("cuda").manual_seed(11))
+    v = torch.tensor(vol, device="cuda", requires_grad=True)
+    l = torch.tensor(lut, device="cuda", requires_grad=True)
+    img = dvr.render(v, l, [p])[0]
+    ((img - target) ** 2).sum().backward()
+    # sample counts per ray from the kernel's workspace
+    L = dvr._lib()
+    work = torch.empty(dvr.workspace_floats([p]), dtype=torch.float32, device="cuda")
+    img2 = torch.empty((64, 64, 3), device="cuda")
+    tr = torch.empty((64, 64), device="cuda")
+    arr, nv = dvr.view_array([p])
+    assert L.mk_dvr_forward(arr, nv, C.c_void_p(v.data_ptr()), C.c_void_p(l.data_ptr()),
+                            C.c_void_p(img2.data_ptr()), C.c_void_p(tr.data_ptr()),
+                            C.c_void_p(work.data_ptr()), None) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(img2, img)
+    counts = work[-64 * 64:].view(torch.int32).view(64, 64)
+    if t_min > 0:
+        assert (tr < t_min).any() and (counts < counts.max()).any()    # some rays stopped early
+    v2 = torch.tensor(vol, device="cuda", requires_grad=True)
+    l2 = torch.tensor(lut, device="cuda", requires_grad=True)
+    ref = torch_reference(v2, l2, p, counts)
+    ((ref - target) ** 2).sum().backward()
+    assert (img - ref).abs().max().item() < 1e-4
+    for name, a, b in (("lut", l.grad, l2.grad), ("volume", v.grad, v2.grad)):
+        rel = ((a - b).norm() / b.norm()).item()
+        print(f"angle {angle} t_min {t_min} {name}: relative error vs torch autograd {rel:.2e}")
+        assert rel < 1e-3
+
+
+def test_batched_views_match_single_views(setup):
+    """One call over views with different cameras, steps and t_min gives each
+    view's image bit for bit and the sum of the per-view gradients."""
+    vol, lut, _, _ = setup
+    views = [dvr.dvr_params(48, 40, view_camera(a), (64, 64, 64), (1, 1, 1), st, tm, 256)
+             for a, st, tm in ((10.0, 0.5, 0.0), (95.0, 0.37, 1e-3), (200.0, 0.8, 0.05))]
+    target = torch.rand((3, 40, 48, 3), device="cuda", generator=torch.Generator("cuda").manual_seed(12))
+    v = torch.tensor(vol, device="cuda", requires_grad=True)
+    l = torch.tensor(lut, device="cuda", requires_grad=True)
+    img = dvr.render(v, l, views)
+    ((img - target) ** 2).sum().backward()
+    gl, gv = torch.zeros_like(l), torch.zeros_like(v)
+    for i, p in enumerate(views):
+        v1 = torch.tensor(vol, device="cuda", requires_grad=True)
+        l1 = torch.tensor(lut, device="cuda", requires_grad=True)
+        im1 = dvr.render(v1, l1, [p])
+        assert torch.equal(im1[0], img[i].detach())
+        ((im1[0] - target[i]) ** 2).sum().backward()
+        gl += l1.grad
+        gv += v1.grad
+    for a, b in ((l.grad, gl), (v.grad, gv)):
+        assert ((a - b).norm() / b.norm()).item() < 1e-5
+
+
+def test_many_views_and_odd_sizes(setup):
+    """35 views (two launches) of a 37x21 image, which no tile divides."""
+    vol, lut, _, _ = setup
+    views = [dvr.dvr_params(37, 21, view_camera(a), (64, 64, 64), (1, 1, 1), 0.6, 0.0, 256)
+             for a in np.arange(35) * 10.3]
+    imgs = dvr.render(torch.tensor(vol, device="cuda"), torch.tensor(lut, device="cuda"), views).cpu().numpy()
+    assert imgs.shape == (35, 21, 37, 3)
+    for i in (0, 31, 32, 34):
+        ref = oracle_forward(views[i], vol.astype(np.float64), lut.astype(np.float64))
+        assert np.abs(imgs[i] - ref).max() < 2e-4
 
 
 def test_invalid_parameters_are_rejected():
@@ -220,3 +262,8 @@ def test_invalid_parameters_are_rejected():
     l = torch.zeros((1, 4), device="cuda")
     with pytest.raises(Exception):
         dvr.render(v, l, [p])
+    a = dvr.dvr_params(8, 8, view_camera(0.0), (4, 4, 4), (1, 1, 1), lut_len=2)
+    b = dvr.dvr_params(16, 8, view_camera(0.0), (4, 4, 4), (1, 1, 1), lut_len=2)
+    l = torch.zeros((2, 4), device="cuda")
+    with pytest.raises(ValueError):
+        dvr.render(v, l, [a, b])
