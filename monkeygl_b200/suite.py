@@ -1,0 +1,271 @@
+"""Per-mode benchmark table of the ray-casting library (``bench.py --suite``).
+
+Rows (synthetic seeded phantoms of monkeygl_b200.phantom):
+  * VR and MIP of the cardiac phantom (int16 512x512x361) at 1024^2, 36 views;
+  * VR of the body phantom (int16 512x512x1559, 4 labels) at 1024^2 with
+    background opacity caps 0.4 and 0.8;
+  * MPR of the cardiac phantom: axial, sagittal, coronal and 8 seeded oblique
+    planes of 512^2, trilinear and nearest, slab of 1 sample;
+  * CPR of a cardiac vessel, 1024 rows x 512 columns, stretched and
+    straightened;
+  * differentiable VR: float32 256^3 volume, 256-entry LUT, 8 views of 256^2,
+    step 0.5 voxel -- forward, backward and their ratio.
+
+Device times are CUDA events on the launching stream around each call, L2
+flushed (256 MiB write) between calls outside the events, median over the
+calls.  "e2e" times are wall clock around the C ABI call with host output.
+Where MonkeyGL's own CUDA path is built (oracle/_ref), its times for the same
+calls are listed beside ours: kernel time for VR/MIP (CUDA events around its
+d_render launch), whole-call wall time for MPR and CPR (its launchers
+allocate, copy and free device memory on every call).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import statistics
+import time
+
+import numpy as np
+
+
+def _median_ms(fn, reps, stream, flush):
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    with torch.cuda.stream(stream):
+        for i in range(reps):
+            flush.zero_()
+            ev[i][0].record(stream)
+            fn(i)
+            ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    return statistics.median(a.elapsed_time(b) for a, b in ev)
+
+
+def _wall_ms(fn, reps):
+    ts = []
+    for i in range(reps):
+        t0 = time.perf_counter()
+        fn(i)
+        ts.append((time.perf_counter() - t0) * 1e3)
+    return statistics.median(ts)
+
+
+def _ref():
+    import oracle
+    return oracle.RefGPU() if oracle.ref_gpu_available() else None
+
+
+def _load_ref(ref, w):
+    ref.set_volume(w.phantom.volume)
+    ref.set_mask(w.phantom.labels)
+    ref.clear_tfs()
+    for l, lut in w.luts.items():
+        ref.set_lut(l, lut)
+
+
+def _workload(ctx, name, bg=0.4):
+    """Workload with the phantom generated once per suite run."""
+    from monkeygl_b200.phantom import config_phantom
+    from monkeygl_b200.workloads import make_workload
+    ph = ctx.setdefault("phantoms", {})
+    if name not in ph:
+        ph[name] = config_phantom(name)
+    return make_workload(name, bg_alpha=bg, phantom=ph[name])
+
+
+def vr_rows(name, bg, rtypes, ctx):
+    import torch
+    from monkeygl_b200 import capi
+    from monkeygl_b200.workloads import view_camera
+    w = _workload(ctx, name, bg)
+    vol = capi.Volume(w.phantom.volume)
+    if w.phantom.labels is not None:
+        vol.set_mask(w.phantom.labels)
+    for l, lut in w.luts.items():
+        vol.set_transfer_function(l, lut)
+    vol.set_label_params(w.label_params)
+    size = 1024
+    out = torch.empty(size * size * 3, dtype=torch.uint8, device="cuda")
+    host = np.empty((size, size, 3), np.uint8)
+    ref = ctx["ref"]
+    if ref is not None:
+        _load_ref(ref, w)
+    rows = []
+    for rt in rtypes:
+        params = [capi.vr_params(size, size, rt, view_camera(a), w.dims, w.spacing) for a in w.angles]
+        n = len(params)
+        stream = ctx["stream"]
+        for i in range(3):
+            vol.render_vr_device(params[i], out.data_ptr(), stream.cuda_stream)
+        ms = _median_ms(lambda i: vol.render_vr_device(params[i % n], out.data_ptr(), stream.cuda_stream),
+                        n, stream, ctx["flush"])
+        e2e = _wall_ms(lambda i: vol.render_vr(params[i % n], out=host), n)
+        row = {"row": f"{'VR' if rt == 0 else 'MIP'} {name}" + (f" bg {bg}" if name == "body" else ""),
+               "image": f"{size}x{size}", "views": n, "ms": round(ms, 4), "fps": round(1e3 / ms, 1),
+               "e2e_ms": round(e2e, 4)}
+        if ref is not None:
+            flats = [np.ascontiguousarray(capi.vr_params_flat(p, w.label_params)) for p in params]
+            pick = sorted({(k * n) // 6 for k in range(6)})
+            rms = statistics.median(ref.kernel_ms(size, size, rt, flats[i], 3) for i in pick)
+            row["ref_kernel_ms"] = round(rms, 4)
+            row["speedup_kernel"] = round(rms / ms, 2)
+        rows.append(row)
+    vol.close()
+    return rows
+
+
+def mpr_rows(ctx):
+    import torch
+    from monkeygl_b200 import capi
+    from monkeygl_b200.workloads import mpr_planes
+    w = _workload(ctx, "cardiac")
+    vol = capi.Volume(w.phantom.volume)
+    planes = mpr_planes(w.phantom, size=512, n_oblique=8)
+    out = torch.empty(512 * 512, dtype=torch.int16, device="cuda")
+    ref = ctx["ref"]
+    if ref is not None:
+        _load_ref(ref, w)
+    rows = []
+    for sampling, sname in ((0, "trilinear"), (1, "nearest")):
+        pp = [capi.plane_params(pl.width, pl.height, 0, sampling, w.spacing, pl.dir_h, pl.dir_v, pl.dir_n,
+                                pl.left_top, pl.pixel_spacing, False, 0.0) for pl in planes]
+        n = len(pp)
+        stream = ctx["stream"]
+        for i in range(3):
+            vol.render_plane_device(pp[i], out.data_ptr(), stream.cuda_stream)
+        ms = _median_ms(lambda i: vol.render_plane_device(pp[i % n], out.data_ptr(), stream.cuda_stream),
+                        4 * n, stream, ctx["flush"])
+        e2e = _wall_ms(lambda i: vol.render_plane(pp[i % n]), 4 * n)
+        row = {"row": f"MPR cardiac {sname}", "image": "512x512", "planes": n, "ms": round(ms, 4),
+               "planes_per_s": round(1e3 / ms, 1), "e2e_ms": round(e2e, 4)}
+        if ref is not None:
+            flats = [capi.plane_params_flat(p) for p in pp]
+            rms = _wall_ms(lambda i: ref.plane(512, 512, flats[i % n], 0, sampling), 2 * n)
+            row["ref_call_ms"] = round(rms, 4)
+            row["speedup_e2e"] = round(rms / e2e, 2)
+        rows.append(row)
+    vol.close()
+    return rows
+
+
+def cpr_rows(ctx):
+    import torch
+    from monkeygl_b200 import capi
+    from monkeygl_b200.workloads import cpr_straightened, cpr_stretched, vessel_path
+    w = _workload(ctx, "cardiac")
+    vol = capi.Volume(w.phantom.volume)
+    path = vessel_path(w.phantom, rows=1024)
+    width = 512
+    out = torch.empty(1024 * width, dtype=torch.int16, device="cuda")
+    ref = ctx["ref"]
+    if ref is not None:
+        _load_ref(ref, w)
+    L = capi.lib()
+    rows = []
+    for builder in (cpr_stretched, cpr_straightened):
+        pts, dirs = builder(path, width)
+        pts = np.ascontiguousarray(pts, np.float64)
+        dirs = np.ascontiguousarray(dirs, np.float64)
+        h = pts.shape[0]
+        stream = ctx["stream"]
+
+        def dev(i):
+            capi._check(L.mk_render_cpr(vol.handle, width, h, pts.ctypes.data_as(C.c_void_p),
+                                        dirs.ctypes.data_as(C.c_void_p), 0, C.c_void_p(out.data_ptr()), 1,
+                                        C.c_void_p(stream.cuda_stream)), "mk_render_cpr")
+
+        for i in range(3):
+            dev(i)
+        ms = _median_ms(dev, 20, stream, ctx["flush"])
+        e2e = _wall_ms(lambda i: vol.render_cpr(width, pts, dirs, False), 20)
+        row = {"row": f"CPR cardiac {builder.__name__.split('_')[1]}", "image": f"{width}x{h}", "ms": round(ms, 4),
+               "e2e_ms": round(e2e, 4)}
+        if ref is not None:
+            rms = _wall_ms(lambda i: ref.cpr(width, pts, dirs, False), 10)
+            row["ref_call_ms"] = round(rms, 4)
+            row["speedup_e2e"] = round(rms / e2e, 2)
+        rows.append(row)
+    vol.close()
+    return rows
+
+
+def dvr_rows(ctx):
+    import torch
+    from monkeygl_b200 import dvr
+    from monkeygl_b200.camera import view_camera
+    from monkeygl_b200.phantom import config_phantom, make_tf_control_points, make_tf_lut
+    ph = config_phantom("diff")
+    vol = np.clip((ph.volume.astype(np.float32) + 1024.0) / 4095.0, 0.0, 1.0).astype(np.float32)
+    rng = np.random.Generator(np.random.PCG64(1337))
+    lut = make_tf_lut(make_tf_control_points(rng))
+    target_lut = make_tf_lut(make_tf_control_points(rng))
+    views = [dvr.dvr_params(256, 256, view_camera(a), (256, 256, 256), (1, 1, 1), 0.5, 1e-4, 256)
+             for a in np.arange(8) * 45.0]
+    v = torch.tensor(vol, device="cuda", requires_grad=True)
+    l = torch.tensor(lut, device="cuda", requires_grad=True)
+    stream = ctx["stream"]
+    with torch.cuda.stream(stream):
+        with torch.no_grad():
+            target = dvr.render(v, torch.tensor(target_lut, device="cuda"), views)
+        fw, bw = [], []
+        for it in range(13):
+            v.grad = None
+            l.grad = None
+            ctx["flush"].zero_()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            img = dvr.render(v, l, views)
+            e1.record(stream)
+            loss = ((img - target) ** 2).mean()
+            loss.backward()
+            e2.record(stream)
+            torch.cuda.synchronize()
+            if it >= 3:
+                fw.append(e0.elapsed_time(e1))
+                bw.append(e1.elapsed_time(e2))
+    # samples per pass from the forward's sample counts
+    work = torch.empty(dvr.workspace_floats(views), dtype=torch.float32, device="cuda")
+    imgs = torch.empty((8, 256, 256, 3), device="cuda")
+    tr = torch.empty((8, 256, 256), device="cuda")
+    arr, nv = dvr.view_array(views)
+    L = dvr._lib()
+    capi_check = dvr._check
+    capi_check(L.mk_dvr_forward(arr, nv, C.c_void_p(v.data_ptr()), C.c_void_p(l.data_ptr()),
+                                C.c_void_p(imgs.data_ptr()), C.c_void_p(tr.data_ptr()), C.c_void_p(work.data_ptr()),
+                                None), "mk_dvr_forward")
+    torch.cuda.synchronize()
+    per = work.numel() // 8
+    samples = sum(int(work[i * per + per - 256 * 256:(i + 1) * per].view(torch.int32).sum().item())
+                  for i in range(8))
+    f, b = statistics.median(fw), statistics.median(bw)
+    return [{"row": "DVR 256^3, 8 views 256^2 (forward)", "ms": round(f, 4), "samples": samples,
+             "gsamples_per_s": round(samples / f / 1e6, 2)},
+            {"row": "DVR 256^3, 8 views 256^2 (backward, LUT + volume)", "ms": round(b, 4),
+             "bwd_over_fwd": round(b / f, 3), "gsamples_per_s": round(samples / b / 1e6, 2)}]
+
+
+def main(args=None):
+    import torch
+    torch.cuda.init()
+    ctx = {"stream": torch.cuda.Stream(), "flush": torch.empty(256 << 20, dtype=torch.uint8, device="cuda"),
+           "ref": _ref()}
+    rows = []
+    rows += vr_rows("cardiac", 0.4, (0, 1), ctx)
+    rows += vr_rows("body", 0.4, (0,), ctx)
+    rows += vr_rows("body", 0.8, (0,), ctx)
+    rows += mpr_rows(ctx)
+    rows += cpr_rows(ctx)
+    rows += dvr_rows(ctx)
+    for r in rows:
+        print(json.dumps(r), flush=True)
+    keys = ["row", "image", "ms", "e2e_ms", "ref_kernel_ms", "ref_call_ms", "speedup_kernel", "speedup_e2e",
+            "bwd_over_fwd", "gsamples_per_s"]
+    print("| " + " | ".join(keys) + " |")
+    print("|" + "---|" * len(keys))
+    for r in rows:
+        print("| " + " | ".join(str(r.get(k, "")) for k in keys) + " |")
+
+
+if __name__ == "__main__":
+    main()
