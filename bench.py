@@ -8,7 +8,8 @@ background cap 0.4, into a 1024x1024 RGB8 image, cycling through 36 views
 (10 degree steps about z).  Synthetic seeded data (monkeygl_b200.workloads).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
-    python bench.py --suite        # per-mode table (VR/MIP/MPR/CPR), not the contract line
+    python bench.py --suite        # per-mode table (VR/MIP/MPR/CPR, differentiable VR), not the contract line
+    python bench.py --serve        # serving: p50/p99 latency and renders/s vs the one-launch-per-request path
 
 `value` is device time of the rendering kernels (CUDA events on the launching
 stream, L2 flushed by a 256 MiB write between steps, outside the events);
@@ -59,6 +60,10 @@ def parse_args():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="body")
     ap.add_argument("--size", type=int, default=1024)
     ap.add_argument("--suite", action="store_true")
+    ap.add_argument("--serve", action="store_true", help="serving benchmark (monkeygl_b200.serve_bench)")
+    ap.add_argument("--serve-requests", type=int, default=10000)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--saturation", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -390,6 +395,10 @@ def main():
     if args.suite:
         from monkeygl_b200 import suite
         suite.main(args)
+        return
+    if args.serve:
+        from monkeygl_b200 import serve_bench
+        serve_bench.main(args)
         return
     if args.impl == "reference":
         # MonkeyGL is one process on one GPU: rank 0 runs it, other ranks exit

@@ -310,6 +310,79 @@ int mk_render_cpr_noalloc(mk_volume vol, int width, int height, const double *po
 /* Wait for all work queued on `stream` (NULL = the volume's stream). */
 int mk_volume_synchronize(mk_volume vol, void *stream);
 
+/* ------------------------------------------------------------------ */
+/* Serving: continuous batching of VR/MIP/MPR requests                 */
+/* ------------------------------------------------------------------ */
+
+/*
+ * No counterpart in MonkeyGL, which serves one request at a time through a
+ * process-wide singleton holding one volume (core/DataManager.cpp:46-54,
+ * server.py).  A server keeps several volumes resident on one device,
+ * admitted against an HBM budget, and renders requests for any of them:
+ * requests take free slots (their LUTs, label parameters, brick visibility
+ * and output buffer), and every step one persistent kernel, launched from a
+ * CUDA graph, pulls 32x8-pixel tiles of all requests in flight from a device
+ * work queue.  A request larger than one step's tile quota spans several
+ * steps; requests arriving meanwhile join the next step.  Each request's
+ * image is the one mk_render_vr / mk_render_plane produce for the same
+ * volume, parameters and tables.  The calls are thread-safe.
+ */
+typedef struct mk_server_s *mk_server;
+
+typedef struct mk_server_config {
+    int device;
+    size_t hbm_budget_bytes;     /* resident volumes + slot buffers; 0 = 90% of the free memory */
+    int max_slots;               /* requests on the device at once, 1..256 */
+    int max_pending;             /* requests waiting for a slot (>= 1); more are refused (MK_ERR_QUEUE_FULL) */
+    int max_pixels;              /* largest image of a request (width * height) */
+    int lut_len;                 /* entries of every LUT of a request, 2..4096 */
+    int max_labels;              /* LUTs per request (labels 0..max_labels-1), 1..65 */
+    int max_bricks;              /* largest volume, in 8^3 bricks; 0 = 512 x 512 x 2048 voxels */
+    int tiles_per_step;          /* tiles of one batched launch; 0 = 8192 */
+} mk_server_config;
+
+enum { MK_REQUEST_VR = 0, MK_REQUEST_MIP = 1, MK_REQUEST_SURFACE = 2, MK_REQUEST_MPR = 3 };
+
+typedef struct mk_request {
+    int volume;                  /* id returned by mk_server_add_volume */
+    int kind;                    /* MK_REQUEST_* */
+    mk_vr_params vr;             /* ray casting (render_type is taken from kind) */
+    mk_plane_params plane;       /* MPR */
+    const float *luts;           /* n_luts tables of lut_len RGBA floats for labels 0..n_luts-1 */
+    int n_luts;                  /* 0..max_labels; labels without a table are transparent */
+    const float *label_params;   /* n_luts rows of (alpha, ww, wl), ww > 0; others (0, 1, 0) */
+    void *out;                   /* host image: W*H*3 (RGB8) or *4 (RGBA8) bytes, W*H int16 for MPR */
+} mk_request;
+
+typedef struct mk_request_times {
+    double submitted_ms;         /* on the server's clock (ms since mk_server_create) */
+    double started_ms;           /* first step holding its tiles was launched */
+    double completed_ms;         /* image copied to `out` */
+} mk_request_times;
+
+typedef struct mk_server_stats {
+    uint64_t submitted, completed, rejected, steps, tiles;
+    size_t resident_bytes, budget_bytes;
+    int volumes, slots_busy, pending;
+} mk_server_stats;
+
+int mk_server_create(const mk_server_config *config, mk_server *out);
+/* Finish the work in flight, then release everything. */
+int mk_server_destroy(mk_server srv);
+/* Upload a volume (and its label volume, or NULL); MK_ERR_BUDGET when it does
+ * not fit the budget beside the volumes already resident. */
+int mk_server_add_volume(mk_server srv, const int16_t *voxels, int dim_x, int dim_y, int dim_z,
+                         const uint8_t *labels, int *volume_id);
+/* MK_ERR_NOT_READY while requests for the volume are queued or in flight. */
+int mk_server_remove_volume(mk_server srv, int volume_id);
+/* Queue a request (its tables are copied); MK_ERR_QUEUE_FULL when max_pending
+ * requests already wait for a slot. */
+int mk_server_submit(mk_server srv, const mk_request *req, uint64_t *ticket);
+/* Wait up to timeout_ms (< 0: no limit) for a request.  MK_OK: the image is
+ * in `out` and the ticket is released; MK_ERR_TIMEOUT: still running. */
+int mk_server_wait(mk_server srv, uint64_t ticket, int timeout_ms, mk_request_times *times);
+int mk_server_get_stats(mk_server srv, mk_server_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,39 @@ class DVRParams(C.Structure):
     ]
 
 
+
+REQUEST_VR, REQUEST_MIP, REQUEST_SURFACE, REQUEST_MPR = 0, 1, 2, 3
+
+
+class ServerConfig(C.Structure):
+    """mk_server_config."""
+    _fields_ = [
+        ("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots", C.c_int),
+        ("max_pending", C.c_int), ("max_pixels", C.c_int), ("lut_len", C.c_int), ("max_labels", C.c_int),
+        ("max_bricks", C.c_int), ("tiles_per_step", C.c_int),
+    ]
+
+
+class Request(C.Structure):
+    """mk_request."""
+    _fields_ = [
+        ("volume", C.c_int), ("kind", C.c_int), ("vr", VRParams), ("plane", PlaneParams),
+        ("luts", C.c_void_p), ("n_luts", C.c_int), ("label_params", C.c_void_p), ("out", C.c_void_p),
+    ]
+
+
+class RequestTimes(C.Structure):
+    _fields_ = [("submitted_ms", C.c_double), ("started_ms", C.c_double), ("completed_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64), ("steps", C.c_uint64),
+        ("tiles", C.c_uint64), ("resident_bytes", C.c_size_t), ("budget_bytes", C.c_size_t),
+        ("volumes", C.c_int), ("slots_busy", C.c_int), ("pending", C.c_int),
+    ]
+
+
 _lib = None
 
 _SIGS = {
@@ -105,6 +138,14 @@ _SIGS = {
     "mk_dvr_workspace_floats": (C.c_int, [C.POINTER(DVRParams), C.c_int, C.POINTER(C.c_size_t)]),
     "mk_dvr_forward": (C.c_int, [C.POINTER(DVRParams), C.c_int] + [C.c_void_p] * 6),
     "mk_dvr_backward": (C.c_int, [C.POINTER(DVRParams), C.c_int] + [C.c_void_p] * 7),
+    "mk_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "mk_server_destroy": (C.c_int, [C.c_void_p]),
+    "mk_server_add_volume": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                       C.POINTER(C.c_int)]),
+    "mk_server_remove_volume": (C.c_int, [C.c_void_p, C.c_int]),
+    "mk_server_submit": (C.c_int, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "mk_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.POINTER(RequestTimes)]),
+    "mk_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
 }
 
 

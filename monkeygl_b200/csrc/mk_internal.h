@@ -104,6 +104,13 @@ float float_bound_above(double c);
 int ensure_device_buffer(VolumeState *v, size_t bytes);
 int ensure_pinned_buffer(VolumeState *v, size_t bytes);
 int rebuild_brick_maps(VolumeState *v, cudaStream_t s);
+// Brick visibility bits and MIP bounds of volume v for the given per-label
+// LUT alpha columns (device pointers, nullptr = no table), LUT lengths and
+// (alpha, ww, wl) rows, written to vis_bits / mip_tmax on stream s.
+int launch_brick_visibility(const VolumeState *v, const float *const *lut_alpha, const int *lut_len,
+                            const float (*params)[3], uint32_t *vis_bits, float *mip_tmax, cudaStream_t s);
+// Words of visibility bits / floats of MIP bounds of a volume's brick maps.
+inline size_t brick_count(const VolumeState *v) { return (size_t)v->nb[0] * v->nb[1] * v->nb[2]; }
 int finish_output(VolumeState *v, void *out, size_t bytes, int out_on_device, cudaStream_t s);
 BrickView brick_view(const VolumeState *v);
 LabelTable label_table(const VolumeState *v);

@@ -24,64 +24,13 @@
 
 #include "mk_internal.h"
 #include "mk_math.h"
+#include "mk_reslice_impl.cuh"
 
 namespace mk {
 
-struct PlaneParams {
-    int W, H;
-    float sp[3];
-    float fdim[3];
-    float h[3], v[3], n[3], lt[3];
-    float ps;
-    int invertZ;
-    float halfNum;
-    int mode;
-    float ww, wl;      // u8 epilogue
-};
-
-template <int MODE>
-__device__ __forceinline__ short reslice_pixel(const PlaneParams &P, cudaTextureObject_t tex, int x,
-                                               int y) {
-    short acc = (MODE == MK_MPR_MIP) ? (short)-32768 : (short)32767;
-    fsum sum = {0.0f, 0.0f};
-    for (float t = -P.halfNum; t <= P.halfNum; t += 1) {
-        const float fLength = t * P.ps;
-        const float pt_x = P.lt[0] + fLength * P.n[0];
-        const float pt_y = P.lt[1] + fLength * P.n[1];
-        const float pt_z = P.lt[2] + fLength * P.n[2];
-        const float fx = (pt_x + x * P.ps * P.h[0] + y * P.ps * P.v[0]) / (P.sp[0] * P.fdim[0]);
-        const float fy = (pt_y + x * P.ps * P.h[1] + y * P.ps * P.v[1]) / (P.sp[1] * P.fdim[1]);
-        float fz = (pt_z + x * P.ps * P.h[2] + y * P.ps * P.v[2]) / (P.sp[2] * P.fdim[2]);
-        // "fz = 1.0 - fz" in double, then rounded to float: identical to the
-        // float subtraction for every float fz (the exact difference rounds once)
-        if (!P.invertZ) fz = 1.0f - fz;
-        const bool inside = fx >= 0 && fx <= 1 && fy >= 0 && fy <= 1 && fz >= 0 && fz <= 1;
-        if (MODE == MK_MPR_AVERAGE) {
-            fsum_add(sum, inside ? 32768 * tex3D<float>(tex, fx, fy, fz) : -32768.0f);
-        } else {
-            const short val = inside ? f2s_sat(32768 * tex3D<float>(tex, fx, fy, fz)) : (short)-32768;
-            if (MODE == MK_MPR_MIP) acc = acc > val ? acc : val;
-            else acc = acc < val ? acc : val;
-        }
-    }
-    if (MODE == MK_MPR_AVERAGE) return fsum_div_to_short(sum, 2 * P.halfNum + 1);
-    return acc;
-}
-
 template <int MODE, bool U8>
 __global__ void __launch_bounds__(256) k_plane(PlaneParams P, cudaTextureObject_t tex, void *out) {
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
-    if (x >= P.W || y >= P.H) return;
-    const short r = reslice_pixel<MODE>(P, tex, x, y);
-    if (U8) {
-        // linear window: 0 at wl - ww/2, 255 at wl + ww/2
-        float g = ((float)r - (P.wl - 0.5f * P.ww)) / P.ww * 255.0f;
-        g = fminf(fmaxf(g, 0.0f), 255.0f);
-        static_cast<uint8_t *>(out)[(size_t)y * P.W + x] = (uint8_t)(g + 0.5f);
-    } else {
-        static_cast<short *>(out)[(size_t)y * P.W + x] = r;
-    }
+    plane_tile<MODE, U8>(P, tex, out, blockIdx.x, blockIdx.y);
 }
 
 // CPR row data: the double point / direction of each row as float pairs.
@@ -111,7 +60,7 @@ __global__ void __launch_bounds__(256) k_cpr(int W, int H, float3 fdim, int inve
     out[(size_t)y * W + x] = r;
 }
 
-static int fill_plane(const VolumeState &v, const mk_plane_params *p, PlaneParams &P) {
+int fill_plane_params(const VolumeState &v, const mk_plane_params *p, PlaneParams &P) {
     if (!p || p->width <= 0 || p->height <= 0 || p->width > 32768 || p->height > 32768) {
         set_last_error("mk_render_plane: plane size must be in [1, 32768]");
         return MK_ERR_INVALID_ARGUMENT;
@@ -164,7 +113,7 @@ extern "C" int mk_render_plane(mk_volume vol, const mk_plane_params *params, int
     }
     VolumeState &v = vol->st;
     PlaneParams P;
-    int rc = fill_plane(v, params, P);
+    int rc = fill_plane_params(v, params, P);
     if (rc != MK_OK) return rc;
     cudaSetDevice(v.device);
     cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
@@ -189,7 +138,7 @@ extern "C" int mk_render_plane_u8(mk_volume vol, const mk_plane_params *params, 
     }
     VolumeState &v = vol->st;
     PlaneParams P;
-    int rc = fill_plane(v, params, P);
+    int rc = fill_plane_params(v, params, P);
     if (rc != MK_OK) return rc;
     P.ww = ww;
     P.wl = wl;

@@ -1,0 +1,82 @@
+// mk_reslice_impl.cuh -- device code of the planar reslice: one output pixel
+// of MonkeyGL's d_renderPlane_{MIP,MinIP,Average} (core/kernel.cu:570-793),
+// shared by the one-plane kernel (mk_reslice.cu) and the serving kernel
+// (mk_server.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mk_internal.h"
+#include "mk_math.h"
+
+namespace mk {
+
+struct PlaneParams {
+    int W, H;
+    float sp[3];
+    float fdim[3];
+    float h[3], v[3], n[3], lt[3];
+    float ps;
+    int invertZ;
+    float halfNum;
+    int mode;
+    float ww, wl;      // u8 epilogue
+};
+
+template <int MODE>
+__device__ __forceinline__ short reslice_pixel(const PlaneParams &P, cudaTextureObject_t tex, int x,
+                                               int y) {
+    short acc = (MODE == MK_MPR_MIP) ? (short)-32768 : (short)32767;
+    fsum sum = {0.0f, 0.0f};
+    // The contraction of MonkeyGL's sums pt + x*ps*h + y*ps*v into fused
+    // multiply-adds is spelled out, left to right: of the fused and unfused
+    // orders, this one reproduces MonkeyGL's kernel pixel for pixel, and
+    // writing it out keeps every kernel that inlines this function on it.
+    const float xs = __fmul_rn((float)x, P.ps), ys = __fmul_rn((float)y, P.ps);
+    for (float t = -P.halfNum; t <= P.halfNum; t += 1) {
+        const float fLength = __fmul_rn(t, P.ps);
+        const float pt_x = __fmaf_rn(fLength, P.n[0], P.lt[0]);
+        const float pt_y = __fmaf_rn(fLength, P.n[1], P.lt[1]);
+        const float pt_z = __fmaf_rn(fLength, P.n[2], P.lt[2]);
+        const float fx = __fdiv_rn(__fmaf_rn(ys, P.v[0], __fmaf_rn(xs, P.h[0], pt_x)), __fmul_rn(P.sp[0], P.fdim[0]));
+        const float fy = __fdiv_rn(__fmaf_rn(ys, P.v[1], __fmaf_rn(xs, P.h[1], pt_y)), __fmul_rn(P.sp[1], P.fdim[1]));
+        float fz = __fdiv_rn(__fmaf_rn(ys, P.v[2], __fmaf_rn(xs, P.h[2], pt_z)), __fmul_rn(P.sp[2], P.fdim[2]));
+        // "fz = 1.0 - fz" in double, then rounded to float: identical to the
+        // float subtraction for every float fz (the exact difference rounds once)
+        if (!P.invertZ) fz = 1.0f - fz;
+        const bool inside = fx >= 0 && fx <= 1 && fy >= 0 && fy <= 1 && fz >= 0 && fz <= 1;
+        if (MODE == MK_MPR_AVERAGE) {
+            fsum_add(sum, inside ? 32768 * tex3D<float>(tex, fx, fy, fz) : -32768.0f);
+        } else {
+            const short val = inside ? f2s_sat(32768 * tex3D<float>(tex, fx, fy, fz)) : (short)-32768;
+            if (MODE == MK_MPR_MIP) acc = acc > val ? acc : val;
+            else acc = acc < val ? acc : val;
+        }
+    }
+    if (MODE == MK_MPR_AVERAGE) return fsum_div_to_short(sum, 2 * P.halfNum + 1);
+    return acc;
+}
+
+// One 32x8 tile (bx, by) of a plane by a 256-thread block: thread t covers
+// pixel (t % 32, t / 32) of the tile.
+template <int MODE, bool U8>
+__device__ __forceinline__ void plane_tile(const PlaneParams &P, cudaTextureObject_t tex, void *out, int bx, int by) {
+    const int x = bx * 32 + (threadIdx.x & 31);
+    const int y = by * 8 + (threadIdx.x >> 5);
+    if (x >= P.W || y >= P.H) return;
+    const short r = reslice_pixel<MODE>(P, tex, x, y);
+    if (U8) {
+        // linear window: 0 at wl - ww/2, 255 at wl + ww/2
+        float g = ((float)r - (P.wl - 0.5f * P.ww)) / P.ww * 255.0f;
+        g = fminf(fmaxf(g, 0.0f), 255.0f);
+        static_cast<uint8_t *>(out)[(size_t)y * P.W + x] = (uint8_t)(g + 0.5f);
+    } else {
+        static_cast<short *>(out)[(size_t)y * P.W + x] = r;
+    }
+}
+
+// Host: kernel parameters of one plane (validates the request).
+int fill_plane_params(const VolumeState &v, const mk_plane_params *p, PlaneParams &P);
+
+}  // namespace mk

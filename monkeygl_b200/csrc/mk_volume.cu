@@ -315,22 +315,28 @@ int finish_output(VolumeState *v, void *out, size_t bytes, int out_on_device, cu
     return MK_OK;
 }
 
-int rebuild_brick_maps(VolumeState *v, cudaStream_t s) {
-    if (!v->maps_dirty) return MK_OK;
+int launch_brick_visibility(const VolumeState *v, const float *const *lut_alpha, const int *lut_len,
+                            const float (*params)[3], uint32_t *vis_bits, float *mip_tmax, cudaStream_t s) {
     const int nbricks = v->nb[0] * v->nb[1] * v->nb[2];
     VisParams P;
     for (int l = 0; l < MK_MAX_LABELS; ++l) {
-        P.lab[l].lut_alpha = v->d_tf_alpha[l];
-        P.lab[l].n = v->tf_len[l];
-        P.lab[l].alpha = v->params[l][0];
-        P.lab[l].ww = v->params[l][1];
-        P.lab[l].wl = v->params[l][2];
+        P.lab[l].lut_alpha = lut_alpha[l];
+        P.lab[l].n = lut_len[l];
+        P.lab[l].alpha = params[l][0];
+        P.lab[l].ww = params[l][1];
+        P.lab[l].wl = params[l][2];
     }
     const int threads = 256;
     const int blocks = (nbricks + threads - 1) / threads;
-    k_brick_visibility<<<blocks, threads, 0, s>>>(v->d_minmax, v->d_labels, nbricks, P,
-                                                  v->d_visible, v->d_mip_tmax);
+    k_brick_visibility<<<blocks, threads, 0, s>>>(v->d_minmax, v->d_labels, nbricks, P, vis_bits, mip_tmax);
     MK_CUDA_TRY(cudaGetLastError());
+    return MK_OK;
+}
+
+int rebuild_brick_maps(VolumeState *v, cudaStream_t s) {
+    if (!v->maps_dirty) return MK_OK;
+    const int rc = launch_brick_visibility(v, v->d_tf_alpha, v->tf_len, v->params, v->d_visible, v->d_mip_tmax, s);
+    if (rc != MK_OK) return rc;
     v->maps_dirty = false;
     return MK_OK;
 }
@@ -603,8 +609,21 @@ extern "C" int mk_volume_set_transfer_function(mk_volume v, int label, const flo
     VolumeState &st = v->st;
     DeviceGuard guard(st.device);
     MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
-    free_tf(st, label);
     st.maps_dirty = true;
+    if (rgba && n_entries > 0 && n_entries == st.tf_len[label] && st.tf_array[label]) {
+        // same length: overwrite the table in place (the texture object stays valid)
+        std::vector<float> alpha(n_entries);
+        for (int i = 0; i < n_entries; ++i) alpha[i] = rgba[4 * i + 3];
+        // on the volume's stream (a plain cudaMemcpy from pageable memory may
+        // return before the data lands, unordered with this non-blocking stream)
+        MK_CUDA_TRY(cudaMemcpy2DToArrayAsync(st.tf_array[label], 0, 0, rgba, n_entries * sizeof(float4),
+                                             n_entries * sizeof(float4), 1, cudaMemcpyHostToDevice, st.stream));
+        MK_CUDA_TRY(cudaMemcpyAsync(st.d_tf_alpha[label], alpha.data(), n_entries * sizeof(float),
+                                    cudaMemcpyHostToDevice, st.stream));
+        MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
+        return MK_OK;
+    }
+    free_tf(st, label);
     if (!rgba || n_entries <= 0) return MK_OK;   // label becomes transparent
     if (n_entries > 65536) {
         set_last_error("mk_volume_set_transfer_function: more than 65536 entries");
@@ -612,8 +631,8 @@ extern "C" int mk_volume_set_transfer_function(mk_volume v, int label, const flo
     }
     cudaChannelFormatDesc cd = cudaCreateChannelDesc<float4>();
     MK_CUDA_TRY(cudaMallocArray(&st.tf_array[label], &cd, n_entries, 1));
-    MK_CUDA_TRY(cudaMemcpy2DToArray(st.tf_array[label], 0, 0, rgba, n_entries * sizeof(float4),
-                                    n_entries * sizeof(float4), 1, cudaMemcpyHostToDevice));
+    MK_CUDA_TRY(cudaMemcpy2DToArrayAsync(st.tf_array[label], 0, 0, rgba, n_entries * sizeof(float4),
+                                         n_entries * sizeof(float4), 1, cudaMemcpyHostToDevice, st.stream));
     cudaResourceDesc rd;
     memset(&rd, 0, sizeof(rd));
     rd.resType = cudaResourceTypeArray;
@@ -628,8 +647,9 @@ extern "C" int mk_volume_set_transfer_function(mk_volume v, int label, const flo
     std::vector<float> alpha(n_entries);
     for (int i = 0; i < n_entries; ++i) alpha[i] = rgba[4 * i + 3];
     MK_CUDA_TRY(cudaMalloc(&st.d_tf_alpha[label], n_entries * sizeof(float)));
-    MK_CUDA_TRY(cudaMemcpy(st.d_tf_alpha[label], alpha.data(), n_entries * sizeof(float),
-                           cudaMemcpyHostToDevice));
+    MK_CUDA_TRY(cudaMemcpyAsync(st.d_tf_alpha[label], alpha.data(), n_entries * sizeof(float),
+                                cudaMemcpyHostToDevice, st.stream));
+    MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
     st.tf_len[label] = n_entries;
     st.device_bytes += (size_t)n_entries * 20;
     return MK_OK;

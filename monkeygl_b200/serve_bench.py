@@ -1,0 +1,194 @@
+"""Serving benchmark (``bench.py --serve``).
+
+Four resident int16 phantoms (256^3; 512x512x361; 512x512x600; 512x512x1559
+with 4 labelled objects) and a seeded Poisson stream of VR / MIP / MPR
+requests (60/20/20) with square images of 256, 512, 768 or 1024 pixels,
+random cameras and transfer functions (workloads.serving_trace).  The same
+trace runs through
+
+  * the server (mk_server_*): requests submitted at their arrival times by
+    one thread, collected by another; latency = completion - arrival;
+  * the plain path: one thread renders each request with the one-frame entry
+    points (set the request's LUTs and label parameters, mk_render_vr /
+    mk_render_plane, synchronous), first come first served; latency =
+    completion - arrival, so time spent waiting behind earlier requests
+    counts.
+
+Then both run the first `--saturation` requests of the trace all at once
+(arrival 0) for the renders/s each path sustains.  Outputs go to pinned host
+buffers in both paths.
+"""
+from __future__ import annotations
+
+import json
+import queue
+import threading
+import time
+
+import numpy as np
+
+
+class _Pool:
+    """Pinned output buffers of the largest image, reused once collected."""
+
+    def __init__(self, n, nbytes):
+        import torch
+        self._t = [torch.empty(nbytes, dtype=torch.uint8, pin_memory=True) for _ in range(n)]
+        self._free = queue.Queue()
+        for i in range(n):
+            self._free.put(i)
+
+    def take(self):
+        return self._free.get()
+
+    def give(self, i):
+        self._free.put(i)
+
+    def view(self, i, shape, dtype):
+        n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        return self._t[i][:n].numpy().view(dtype).reshape(shape)
+
+
+def _shape(r):
+    from . import capi
+    if r.kind == capi.REQUEST_MPR:
+        return (r.size, r.size), np.int16
+    return (r.size, r.size, 3), np.uint8
+
+
+def _pcts(lat):
+    a = np.asarray(lat, np.float64)
+    return {"p50_ms": round(float(np.percentile(a, 50)), 3), "p99_ms": round(float(np.percentile(a, 99)), 3),
+            "mean_ms": round(float(a.mean()), 3), "max_ms": round(float(a.max()), 3)}
+
+
+def run_server(srv, vids, trace, pool, open_loop: bool):
+    """Submit the trace (at its arrival times if open_loop, else at once);
+    returns per-request latencies (ms), wall seconds and the images' tickets order."""
+    from . import server as S
+    q = queue.Queue()
+    t0 = time.perf_counter()
+
+    def submitter():
+        for i, r in enumerate(trace):
+            if open_loop:
+                dt = t0 + r.arrival_s - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+            b = pool.take()
+            shape, dt_ = _shape(r)
+            sub_wall = time.perf_counter()
+            t = S.submit_request(srv, vids[r.volume], r, out=pool.view(b, shape, dt_))
+            q.put((i, t, b, sub_wall))
+        q.put(None)
+
+    th = threading.Thread(target=submitter, daemon=True)
+    th.start()
+    lat = [0.0] * len(trace)
+    last = t0
+    while True:
+        item = q.get()
+        if item is None:
+            break
+        i, t, b, sub_wall = item
+        _, tm = srv.wait(t)
+        pool.give(b)
+        late = max(0.0, sub_wall - (t0 + trace[i].arrival_s)) * 1e3 if open_loop else (sub_wall - t0) * 1e3
+        lat[i] = late + (tm["completed_ms"] - tm["submitted_ms"])
+        last = time.perf_counter()
+    th.join()
+    return lat, last - t0
+
+
+def run_plain(vols, trace, pool, open_loop: bool):
+    from . import server as S
+    b = pool.take()
+    lat = []
+    t0 = time.perf_counter()
+    for r in trace:
+        if open_loop:
+            dt = t0 + r.arrival_s - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+        shape, dt_ = _shape(r)
+        S.render_plain(vols[r.volume], r, out=pool.view(b, shape, dt_))
+        lat.append((time.perf_counter() - (t0 + (r.arrival_s if open_loop else 0.0))) * 1e3)
+    wall = time.perf_counter() - t0
+    pool.give(b)
+    return lat, wall
+
+
+def main(args):
+    import torch
+    from . import capi
+    from . import server as S
+    from .phantom import make_phantom
+    from .workloads import SERVING_VOLUMES, serving_trace
+
+    n = getattr(args, "serve_requests", 10000) or 10000
+    rate = getattr(args, "serve_rate", 200.0) or 200.0
+    nsat = min(n, getattr(args, "saturation", 2000) or 2000)
+    torch.cuda.init()
+    phantoms = [make_phantom(d, s, seed, with_labels=lab) for d, s, seed, lab in SERVING_VOLUMES]
+    specs = [(p.dims, p.spacing, p.labels is not None) for p in phantoms]
+    trace = serving_trace(specs, n, rate, seed=2024)
+    pool = _Pool(64, 1024 * 1024 * 4)
+
+    srv = S.Server(max_slots=32, max_pending=max(n, 1), max_pixels=1024 * 1024, max_labels=8)
+    vids = [srv.add_volume(p.volume, p.labels) for p in phantoms]
+    plain_vols = []
+    for p in phantoms:
+        v = capi.Volume(p.volume)
+        if p.labels is not None:
+            v.set_mask(p.labels)
+        plain_vols.append(v)
+
+    # warm-up: every volume and kind once on both paths; spot-check equality
+    warm = serving_trace(specs, 64, 1000.0, seed=99)
+    bad = []
+    for i, r in enumerate(warm):
+        shape, dt = _shape(r)
+        b1, b2 = pool.take(), pool.take()
+        out1, out2 = pool.view(b1, shape, dt), pool.view(b2, shape, dt)
+        srv.wait(S.submit_request(srv, vids[r.volume], r, out=out1))
+        S.render_plain(plain_vols[r.volume], r, out=out2)
+        if not np.array_equal(out1, out2):
+            d = np.abs(out1.astype(np.int64) - out2.astype(np.int64))
+            bad.append({"request": i, "kind": r.kind, "volume": r.volume, "size": r.size,
+                        "pixels_differing": int((d.reshape(r.size, r.size, -1).max(-1) > 0).sum()),
+                        "max_diff": int(d.max())})
+        pool.give(b1)
+        pool.give(b2)
+    if bad:
+        print(json.dumps({"mismatches": bad}), flush=True)
+        raise RuntimeError(f"server and plain path images differ on {len(bad)} of {len(warm)} requests")
+
+    st0 = srv.stats()
+    lat_s, wall_s = run_server(srv, vids, trace, pool, open_loop=True)
+    st1 = srv.stats()
+    lat_p, wall_p = run_plain(plain_vols, trace, pool, open_loop=True)
+    sat_s_lat, sat_s = run_server(srv, vids, trace[:nsat], pool, open_loop=False)
+    sat_p_lat, sat_p = run_plain(plain_vols, trace[:nsat], pool, open_loop=False)
+    srv.close()
+    for v in plain_vols:
+        v.close()
+
+    kinds = {0: "VR", 1: "MIP", 3: "MPR"}
+    mix = {k: sum(1 for r in trace if r.kind == c) for c, k in kinds.items()}
+    line = {
+        "metric": "served latency p50/p99 (ms) at the arrival rate, and renders/s at saturation",
+        "workload": f"{n} requests, Poisson {rate:g}/s, VR/MIP/MPR {mix}, sizes 256..1024^2, 4 resident volumes "
+                    "(256^3, 512^2x361, 512^2x600, 512^2x1559 + labels), random cameras and TFs",
+        "server": {**_pcts(lat_s), "renders_per_s": round(n / wall_s, 1),
+                   "saturation_renders_per_s": round(nsat / sat_s, 1),
+                   "steps": st1["steps"] - st0["steps"], "tiles": st1["tiles"] - st0["tiles"],
+                   "resident_mb": round(st1["resident_bytes"] / 2 ** 20, 1)},
+        "plain": {**_pcts(lat_p), "renders_per_s": round(n / wall_p, 1),
+                  "saturation_renders_per_s": round(nsat / sat_p, 1)},
+        "saturation_requests": nsat,
+        "saturation_ratio": round((nsat / sat_s) / (nsat / sat_p), 2),
+        "p99_target_ms": 20.0,
+    }
+    line["saturation_latency"] = {"server": _pcts(sat_s_lat), "plain": _pcts(sat_p_lat)}
+    print(json.dumps(line), flush=True)
+    return line

@@ -180,3 +180,86 @@ def cpr_stretched(path: np.ndarray, width: int) -> tuple:
     dirs = np.tile(d, (len(path), 1))
     pts = path - dirs * (width / 2.0)
     return pts, dirs
+
+
+# ----------------------------------------------------------------------
+# Serving trace
+
+# Resident volumes of the serving workload: (dims, spacing, seed, labels).
+SERVING_VOLUMES = [
+    ((256, 256, 256), (1.0, 1.0, 1.0), 2001, False),
+    ((512, 512, 361), (0.351, 0.351, 0.3), 1235, False),
+    ((512, 512, 600), (0.7, 0.7, 0.8), 2003, False),
+    ((512, 512, 1559), (0.7422, 0.7422, 1.0), 1236, True),
+]
+
+
+@dataclass
+class ServingRequest:
+    arrival_s: float
+    volume: int                      # index into the volume list
+    kind: int                        # capi.REQUEST_VR / _MIP / _MPR
+    size: int
+    vr: object = None                # capi.VRParams
+    plane: object = None             # capi.PlaneParams
+    luts: np.ndarray | None = None   # (n, 256, 4) float32, labels 0..n-1
+    label_params: np.ndarray | None = None   # (n, 3) alpha, ww, wl
+
+
+def random_plane(dims, spacing, size: int, rng, sampling: int = 0):
+    """Oblique plane through the volume centre +-10% of the extent: unit
+    normal uniform on the sphere, random in-plane rotation, size x size at
+    the minimum spacing, slab of one sample."""
+    from . import capi
+    ext = np.array(dims, np.float64) * np.array(spacing, np.float64)
+    ps = float(min(spacing))
+    n = rng.standard_normal(3)
+    n /= np.linalg.norm(n)
+    a = np.cross(n, [1.0, 0, 0] if abs(n[0]) < 0.9 else [0, 1.0, 0])
+    a /= np.linalg.norm(a)
+    b = np.cross(n, a)
+    th = rng.uniform(0, 2 * np.pi)
+    h = np.cos(th) * a + np.sin(th) * b
+    v = np.cross(n, h)
+    c = ext / 2.0 + rng.uniform(-0.1, 0.1, 3) * ext
+    lt = c - h * (0.5 * size * ps) - v * (0.5 * size * ps)
+    return capi.plane_params(size, size, capi.MPR_AVERAGE, sampling, spacing, h, v, np.cross(h, v), lt, ps, False, 0.0)
+
+
+def serving_trace(volumes, n: int, rate: float, seed: int = 77, sizes=(256, 512, 768, 1024),
+                  mix=(0.6, 0.2, 0.2)) -> list:
+    """n requests with Poisson arrivals at `rate` per second over `volumes`
+    (list of (dims, spacing, has_labels)): VR / MIP / MPR in proportions
+    `mix`, square images of a size drawn from `sizes`, random cameras
+    (rotation about z and x, zoom 0.8-1.5) and random transfer functions
+    (one 4-point piecewise-linear LUT per label, opacity caps U(0.6, 1) on
+    labelled objects and U(0.3, 1) on the background), random oblique planes
+    with trilinear or nearest sampling."""
+    from . import capi
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out, t = [], 0.0
+    for _ in range(n):
+        t += rng.exponential(1.0 / rate)
+        vi = int(rng.integers(len(volumes)))
+        dims, spacing, labelled = volumes[vi]
+        u = rng.random()
+        kind = capi.REQUEST_VR if u < mix[0] else capi.REQUEST_MIP if u < mix[0] + mix[1] else capi.REQUEST_MPR
+        size = int(sizes[int(rng.integers(len(sizes)))])
+        if kind == capi.REQUEST_MPR:
+            plane = random_plane(dims, spacing, size, rng, sampling=int(rng.integers(2)))
+            out.append(ServingRequest(t, vi, kind, size, plane=plane))
+            continue
+        c = cam.Camera()
+        c.anterior()
+        c.rotate(float(rng.uniform(0.0, 360.0)), float(rng.uniform(-40.0, 40.0)))
+        c.zoom(float(rng.uniform(0.8, 1.5)))
+        vr = capi.vr_params(size, size, kind, c, dims, spacing)
+        nl = 5 if labelled else 1
+        luts = np.stack([make_tf_lut(make_tf_control_points(rng)) for _ in range(nl)])
+        lp = np.zeros((nl, 3), np.float32)
+        lp[:, 1] = WW
+        lp[:, 2] = WL
+        lp[0, 0] = rng.uniform(0.3, 1.0) if labelled else 1.0
+        lp[1:, 0] = rng.uniform(0.6, 1.0, nl - 1)
+        out.append(ServingRequest(t, vi, kind, size, vr=vr, luts=luts, label_params=lp))
+    return out

@@ -6,11 +6,13 @@
 // MonkeyGL's own HelloMonkey API can be read back on a machine without a GPU.
 // tests/golden/make_host_golden.py drives this through the mkrh_* functions.
 #include <malloc.h>
+#include <stdlib.h>
 #include <string.h>
 #include <unistd.h>
 
 #include <map>
 #include <memory>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -146,12 +148,23 @@ extern "C" void cu_renderCPR(short *pData, int width, int height, cudaTextureObj
 // (core/MarchingCube.cpp:298), so mkrh_create takes the directory that holds
 // resources/ and constructs the object from there.
 
-// mkrh_zero_heap(1) makes every allocation of 64 KiB or more come from fresh
-// (zero-filled) pages.  MonkeyGL's VolumeInfo::AddNewObjectMask allocates the
-// label volume with new[] and never clears it (core/VolumeInfo.cpp:96-104);
-// recycled heap memory there leaves labels above 64 outside every mask, which
-// its kernel then uses to index 65-entry tables.  With fresh pages the label
-// volume starts at zero, as MonkeyGL evidently assumes.
+// Array allocations of MonkeyGL's host code in this library come zero-filled:
+// the library is linked with -Bsymbolic-functions, so MonkeyGL's new[] binds
+// to this definition.  MonkeyGL allocates its label volume with new[] and
+// never clears it (core/VolumeInfo.cpp:96-104); recycled heap memory there
+// leaves labels above 64 outside every mask, which its kernel then uses to
+// index 65-entry tables.  Zero-filled, the label volume starts at zero, as
+// MonkeyGL evidently assumes, whatever the process allocated before.
+void *operator new[](size_t n) {
+    void *p = calloc(1, n ? n : 1);
+    if (!p) throw std::bad_alloc();
+    return p;
+}
+void operator delete[](void *p) noexcept { free(p); }
+void operator delete[](void *p, size_t) noexcept { free(p); }
+
+// mkrh_zero_heap(1) also makes allocations of 64 KiB or more come from fresh
+// pages (a second line of defence for allocations not made with new[]).
 extern "C" int mkrh_zero_heap(int on) {
     return on ? mallopt(M_MMAP_THRESHOLD, 64 * 1024) : 1;
 }

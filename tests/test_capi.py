@@ -110,3 +110,30 @@ def test_dvr_host_validation():
                             None) == capi.MK_ERR_INVALID_ARGUMENT
     assert L.mk_dvr_backward(arr, nv, C.c_void_p(16), C.c_void_p(16), None, C.c_void_p(16), C.c_void_p(16),
                              None, None) == capi.MK_ERR_INVALID_ARGUMENT
+
+
+def test_server_host_validation():
+    """mk_server_create validates its configuration before touching a device
+    and reports a machine without one as MK_ERR_NO_DEVICE."""
+    L = capi.lib()
+    h = C.c_void_p()
+
+    def cfg(**kw):
+        c = capi.ServerConfig()
+        c.device, c.hbm_budget_bytes, c.max_slots, c.max_pending = 0, 0, 8, 16
+        c.max_pixels, c.lut_len, c.max_labels, c.max_bricks, c.tiles_per_step = 1 << 20, 256, 8, 0, 0
+        for k, v in kw.items():
+            setattr(c, k, v)
+        return c
+
+    for bad in (dict(max_slots=0), dict(max_slots=257), dict(max_pending=0), dict(lut_len=1), dict(lut_len=5000),
+                dict(max_labels=0), dict(max_labels=66), dict(max_pixels=0), dict(tiles_per_step=-1)):
+        assert L.mk_server_create(C.byref(cfg(**bad)), C.byref(h)) == capi.MK_ERR_INVALID_ARGUMENT, bad
+    assert L.mk_server_create(None, C.byref(h)) == capi.MK_ERR_INVALID_ARGUMENT
+    n = C.c_int(-1)
+    L.mk_device_count(C.byref(n))
+    if n.value == 0:
+        assert L.mk_server_create(C.byref(cfg()), C.byref(h)) == capi.MK_ERR_NO_DEVICE
+    for fn, args in (("mk_server_destroy", (None,)), ("mk_server_remove_volume", (None, 1)),
+                     ("mk_server_get_stats", (None, None)), ("mk_server_wait", (None, 1, 0, None))):
+        assert getattr(L, fn)(*args) == capi.MK_ERR_INVALID_ARGUMENT, fn
