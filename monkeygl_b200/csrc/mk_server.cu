@@ -19,9 +19,11 @@
 //    per resident slot of the device, each pulling tiles with an atomic
 //    counter until the list is exhausted (no waiting on other blocks or on
 //    the host).  A request spans steps when it has more tiles than a step
-//    takes; requests admitted meanwhile join the next step.  Two steps are in
-//    flight at a time; finished images go back on a copy stream behind the
-//    step that finished them.
+//    takes; requests admitted meanwhile join the next step.  Steps alternate
+//    between two streams, so the next step's tiles fill the tail of the one
+//    before (a step ends with its slowest tile); up to four are in flight.
+//    Finished images go back on a copy stream behind the steps that hold
+//    their tiles.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -170,7 +172,12 @@ using namespace mk;
 struct mk_server_s {
     mk_server_config cfg;
     int blocks = 0;
-    cudaStream_t stream = nullptr, copy_stream = nullptr;
+    cudaStream_t stream = nullptr;                 // admissions: tables, descriptors, brick visibility
+    cudaStream_t step_stream[2] = {};              // steps alternate, so one fills the other's tail
+    cudaStream_t copy_stream = nullptr;            // finished images to the host
+    cudaEvent_t uploaded = nullptr;                // after the latest admissions
+    bool uploads_pending = false;
+    cudaEvent_t last_kernel[2] = {};               // latest step kernel on each step stream
     std::vector<Slot> slots;
     SlotDesc *d_slots = nullptr, *h_slots = nullptr;
     int *d_queue[2] = {}, *h_queue[2] = {}, *d_next[2] = {};
@@ -211,6 +218,7 @@ void release(mk_server_s *s) {
         if (s->h_queue[b]) cudaFreeHost(s->h_queue[b]);
         if (s->d_next[b]) cudaFree(s->d_next[b]);
         if (s->queue_free[b]) cudaEventDestroy(s->queue_free[b]);
+        if (s->last_kernel[b]) cudaEventDestroy(s->last_kernel[b]);
     }
     for (auto &e : s->event_pool) {
         cudaEventDestroy(e.first);
@@ -232,7 +240,10 @@ void release(mk_server_s *s) {
     if (s->d_slots) cudaFree(s->d_slots);
     if (s->h_slots) cudaFreeHost(s->h_slots);
     for (auto &kv : s->volumes) mk_volume_destroy(kv.second.vol);
+    if (s->uploaded) cudaEventDestroy(s->uploaded);
     if (s->stream) cudaStreamDestroy(s->stream);
+    for (int b = 0; b < 2; ++b)
+        if (s->step_stream[b]) cudaStreamDestroy(s->step_stream[b]);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
 }
 
@@ -318,6 +329,7 @@ int admit(mk_server_s *s, uint64_t ticket, int slot_index) {
         D.bv.nbz = vs.nb[2];
     }
     MK_CUDA_TRY(cudaMemcpyAsync(s->d_slots + slot_index, &D, sizeof(SlotDesc), cudaMemcpyHostToDevice, s->stream));
+    s->uploads_pending = true;
     sl.ticket = ticket;
     q.slot = slot_index;
     return MK_OK;
@@ -350,15 +362,25 @@ int issue_step(mk_server_s *s) {
     if (n == 0) return MK_OK;
     s->h_queue[b][0] = n;
     s->h_queue[b][1] = 0;
+    cudaStream_t ss = s->step_stream[b];
+    if (s->uploads_pending) {                              // descriptors and maps of new requests first
+        MK_CUDA_TRY(cudaEventRecord(s->uploaded, s->stream));
+        s->uploads_pending = false;
+    }
+    MK_CUDA_TRY(cudaStreamWaitEvent(ss, s->uploaded, 0));
     MK_CUDA_TRY(cudaMemcpyAsync(s->d_queue[b], s->h_queue[b], 8 + (size_t)n * sizeof(TileItem),
-                                cudaMemcpyHostToDevice, s->stream));
-    MK_CUDA_TRY(cudaEventRecord(s->queue_free[b], s->stream));
-    MK_CUDA_TRY(cudaGraphLaunch(s->graph_exec[b], s->stream));
+                                cudaMemcpyHostToDevice, ss));
+    MK_CUDA_TRY(cudaEventRecord(s->queue_free[b], ss));
+    MK_CUDA_TRY(cudaGraphLaunch(s->graph_exec[b], ss));
     const auto ev = s->event_pool[s->step_count % s->event_pool.size()];
     st.kernel_done = ev.first;
     st.copies_done = ev.second;
-    MK_CUDA_TRY(cudaEventRecord(st.kernel_done, s->stream));
+    MK_CUDA_TRY(cudaEventRecord(st.kernel_done, ss));
+    // A finishing request's earlier tiles are in earlier steps: those on this
+    // stream are ordered before this one, the other stream's latest may still run.
     MK_CUDA_TRY(cudaStreamWaitEvent(s->copy_stream, st.kernel_done, 0));
+    MK_CUDA_TRY(cudaStreamWaitEvent(s->copy_stream, s->last_kernel[b ^ 1], 0));
+    MK_CUDA_TRY(cudaEventRecord(s->last_kernel[b], ss));
     for (uint64_t t : st.finishing) {
         Req &q = s->reqs[t];
         Slot &sl = s->slots[q.slot];
@@ -433,8 +455,8 @@ void worker_loop(mk_server_s *s) {
             s->active.push_back(t);
             progressed = true;
         }
-        // 3. keep two steps in flight
-        if (rc == MK_OK && s->inflight.size() < 2) {
+        // 3. keep up to four steps in flight
+        if (rc == MK_OK && s->inflight.size() < 4) {
             bool work = false;
             for (uint64_t t : s->active) {
                 const Req &q = s->reqs[t];
@@ -538,7 +560,11 @@ extern "C" int mk_server_create(const mk_server_config *config, mk_server *out) 
     AllocInjector dev_alloc;
     do {
         if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) break;
+        if ((e = cudaStreamCreateWithFlags(&s->step_stream[0], cudaStreamNonBlocking)) != cudaSuccess) break;
+        if ((e = cudaStreamCreateWithFlags(&s->step_stream[1], cudaStreamNonBlocking)) != cudaSuccess) break;
         if ((e = cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) break;
+        if ((e = cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming)) != cudaSuccess) break;
+        if ((e = cudaEventRecord(s->uploaded, s->stream)) != cudaSuccess) break;
         s->slots.resize(c.max_slots);
         cudaChannelFormatDesc cd = cudaCreateChannelDesc<float4>();
         for (auto &sl : s->slots) {
@@ -574,10 +600,12 @@ extern "C" int mk_server_create(const mk_server_config *config, mk_server *out) 
             if ((e = cudaMallocHost(&s->h_queue[b], qbytes)) != cudaSuccess) break;
             if ((e = dev_alloc((void **)&s->d_next[b], sizeof(int))) != cudaSuccess) break;
             if ((e = cudaEventCreateWithFlags(&s->queue_free[b], cudaEventDisableTiming)) != cudaSuccess) break;
-            e = cudaEventRecord(s->queue_free[b], s->stream);
+            if ((e = cudaEventRecord(s->queue_free[b], s->step_stream[b])) != cudaSuccess) break;
+            if ((e = cudaEventCreateWithFlags(&s->last_kernel[b], cudaEventDisableTiming)) != cudaSuccess) break;
+            e = cudaEventRecord(s->last_kernel[b], s->step_stream[b]);
         }
         if (e != cudaSuccess) break;
-        for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+        for (int i = 0; i < 8 && e == cudaSuccess; ++i) {
             cudaEvent_t a = nullptr, b2 = nullptr;
             if ((e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming)) != cudaSuccess) break;
             if ((e = cudaEventCreateWithFlags(&b2, cudaEventDisableTiming)) != cudaSuccess) {
@@ -632,6 +660,8 @@ extern "C" int mk_server_destroy(mk_server s) {
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->cfg.device);
     cudaStreamSynchronize(s->stream);
+    cudaStreamSynchronize(s->step_stream[0]);
+    cudaStreamSynchronize(s->step_stream[1]);
     cudaStreamSynchronize(s->copy_stream);
     release(s);
     delete s;
