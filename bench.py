@@ -71,20 +71,27 @@ def parse_args():
 # ----------------------------------------------------------------------
 # process group (one process per GPU)
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend="nccl"):
+    """Rank, local rank and world size from the torchrun environment; joins
+    the process group when there is more than one rank.  `backend` "gloo"
+    runs the same host logic without GPUs."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     import torch
+    if backend == "nccl":
+        torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(local)
+        kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
     return rank, local, world
+
+
+def _reduce_device():
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
 
 
 def barrier(world):
@@ -98,9 +105,15 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_views(angles, rank):
+    """The views a rank renders, in order: every view, starting 7 views
+    further along per rank so the replicas do not render in lockstep."""
+    return [angles[(rank * 7 + i) % len(angles)] for i in range(len(angles))]
 
 
 def sum_over_ranks(x, world):
@@ -108,7 +121,7 @@ def sum_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_reduce_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -211,16 +224,16 @@ def frame_params(w, angle, size, render_type=0):
     return capi.vr_params(size, size, render_type, view_camera(angle), w.dims, w.spacing, invert_z=False)
 
 
-def cpu_baseline(w, angle, size, rank_views=1):
-    """Time the C restatement (oracle, texture-emulating FP32) on a strided
-    sample of rows with every host thread; scale to frames per second."""
+def cpu_baseline(w, angle, size):
+    """Time the C restatement (oracle, texture-emulating FP32): whole frames
+    of consecutive views with OpenMP over rows on every host thread for about
+    10 s, and one thread on every 16th row of a frame (scaled to a frame)."""
     import oracle
     from monkeygl_b200 import capi
     cv = oracle.CpuVolume(w.phantom.volume, w.phantom.labels)
     for l, lut in w.luts.items():
         cv.set_lut(l, lut)
     cores = os.cpu_count() or 1
-    # whole frames, cycling through the views, until about 10 s have elapsed
     frames, t0 = 0, time.perf_counter()
     angles = list(w.angles)
     start = angles.index(angle) if angle in angles else 0
@@ -232,10 +245,16 @@ def cpu_baseline(w, angle, size, rank_views=1):
         dt = time.perf_counter() - t0
         if dt >= 10.0 or frames >= 2 * len(angles):
             break
+    flat = capi.vr_params_flat(frame_params(w, angles[start], size), w.label_params)
+    t1 = time.perf_counter()
+    cv.render_vr_rows(size, size, 0, flat, 0, 16, size // 16, threads=1)
+    one = (time.perf_counter() - t1) * 16
     return {"value": round(frames / dt, 4), "unit": "fps", "cores": cores, "kind": "port",
+            "single_thread_fps": round(1.0 / one, 5),
             "sample": f"oracle/mk_oracle.c (FP32, texture emulation, OpenMP over rows) rendering {frames} "
                       f"full {size}x{size} frames of consecutive views from {angle:.0f} deg in "
-                      f"{dt:.1f} s on {cores} host threads"}
+                      f"{dt:.1f} s on {cores} host threads; single thread: every 16th row of one frame, "
+                      f"{one:.1f} s per frame"}
 
 
 def run_mine(args, rank, local, world):
@@ -247,7 +266,7 @@ def run_mine(args, rank, local, world):
     size = args.size
     vol = setup_volume(w, local)
     angles = w.angles
-    views = [angles[(rank * 7 + i) % len(angles)] for i in range(len(angles))]
+    views = rank_views(angles, rank)
     params = [frame_params(w, a, size) for a in views]
     stream = torch.cuda.Stream()
     out = torch.empty(size * size * 3, dtype=torch.uint8, device="cuda")
@@ -393,8 +412,10 @@ def run_reference(args, rank, world):
 def main():
     args = parse_args()
     if args.suite:
+        import oracle
         from monkeygl_b200 import suite
-        suite.main(args)
+        # MonkeyGL's own kernels built from its sources (oracle/_ref), for the reference columns
+        suite.main(args, oracle.RefGPU() if oracle.ref_gpu_available() else None)
         return
     if args.serve:
         from monkeygl_b200 import serve_bench

@@ -14,7 +14,7 @@ Rows (synthetic seeded phantoms of monkeygl_b200.phantom):
 Device times are CUDA events on the launching stream around each call, L2
 flushed (256 MiB write) between calls outside the events, median over the
 calls.  "e2e" times are wall clock around the C ABI call with host output.
-Where MonkeyGL's own CUDA path is built (oracle/_ref), its times for the same
+Where the caller supplies MonkeyGL's own CUDA path, its times for the same
 calls are listed beside ours: kernel time for VR/MIP (CUDA events around its
 d_render launch), whole-call wall time for MPR and CPR (its launchers
 allocate, copy and free device memory on every call).
@@ -49,11 +49,6 @@ def _wall_ms(fn, reps):
         fn(i)
         ts.append((time.perf_counter() - t0) * 1e3)
     return statistics.median(ts)
-
-
-def _ref():
-    import oracle
-    return oracle.RefGPU() if oracle.ref_gpu_available() else None
 
 
 def _load_ref(ref, w):
@@ -245,11 +240,14 @@ def dvr_rows(ctx):
              "bwd_over_fwd": round(b / f, 3), "gsamples_per_s": round(samples / b / 1e6, 2)}]
 
 
-def main(args=None):
+def main(args=None, ref=None):
+    """Print the table.  `ref` is MonkeyGL's own CUDA path (an object with
+    set_volume / set_mask / clear_tfs / set_lut / kernel_ms / plane / cpr),
+    supplied by the caller, or None for no reference columns."""
     import torch
     torch.cuda.init()
     ctx = {"stream": torch.cuda.Stream(), "flush": torch.empty(256 << 20, dtype=torch.uint8, device="cuda"),
-           "ref": _ref()}
+           "ref": ref}
     rows = []
     rows += vr_rows("cardiac", 0.4, (0, 1), ctx)
     rows += vr_rows("body", 0.4, (0,), ctx)
