@@ -80,6 +80,15 @@ struct VolumeState {
     size_t h_pinned_bytes = 0;
     unsigned long long *d_counter = nullptr;
 
+    // launch orders of the ray-casting tiles (centre first), per image size
+    // and pan: {W, H, x pan, y pan} -> device table of tile indices
+    struct TileOrder {
+        int key[4];
+        int *d_tiles;
+    };
+    TileOrder orders[16] = {};
+    int n_orders = 0;
+
     size_t device_bytes = 0;
 };
 

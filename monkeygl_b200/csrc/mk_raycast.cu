@@ -37,16 +37,24 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <utility>
+#include <vector>
+
 #include "mk_internal.h"
 #include "mk_math.h"
 #include "mk_raycast_impl.cuh"
 
 namespace mk {
 
+// One 32x8 tile per block.  With `order`, block i renders tile order[i]
+// (index by * tiles_x + bx): the launch takes tiles centre first, where the
+// projected volume -- and the longest rays -- usually are, so they start in
+// the first wave instead of forming the tail of the launch.
 template <int MODE, int TRACK, bool COUNT>
 __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_t vol,
                                                  cudaTextureObject_t mask, LabelTable LT,
-                                                 BrickView BV) {
+                                                 BrickView BV, const int *__restrict__ order) {
     __shared__ LabelSmem S;
     __shared__ float s_acc[TRACK == kTrackShared ? kMaxTrackedLabels : 1][256];
     __shared__ uint8_t s_px[8][32 * 3];
@@ -54,29 +62,83 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
     load_label_smem(S, LT, TRACK);
     if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
-    raycast_tile<MODE, TRACK, COUNT>(P, vol, mask, S, BV, s_acc, s_px, &s_count, blockIdx.x, blockIdx.y);
+    int bx = blockIdx.x, by = blockIdx.y;
+    if (order) {
+        const int t = order[blockIdx.x], tx = (P.W + 31) / 32;
+        bx = t % tx;
+        by = t / tx;
+    }
+    raycast_tile<MODE, TRACK, COUNT>(P, vol, mask, S, BV, s_acc, s_px, &s_count, bx, by);
 }
 
 template <int MODE, int TRACK, bool COUNT>
 static void launch_mode(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
-                        const LabelTable &LT, const BrickView &BV, cudaStream_t s) {
-    dim3 grid((P.W + 31) / 32, (P.H + 7) / 8);
-    k_raycast<MODE, TRACK, COUNT><<<grid, 256, 0, s>>>(P, vol, mask, LT, BV);
+                        const LabelTable &LT, const BrickView &BV, const int *order, cudaStream_t s) {
+    const int tx = (P.W + 31) / 32, ty = (P.H + 7) / 8;
+    const dim3 grid = order ? dim3(tx * ty) : dim3(tx, ty);
+    k_raycast<MODE, TRACK, COUNT><<<grid, 256, 0, s>>>(P, vol, mask, LT, BV, order);
 }
 
 template <bool COUNT>
 static void launch_raycast(int mode, int track, const RayParams &P, cudaTextureObject_t vol,
                            cudaTextureObject_t mask, const LabelTable &LT, const BrickView &BV,
-                           cudaStream_t s) {
+                           const int *order, cudaStream_t s) {
     if (mode == kModeVR) {
-        if (track == kTrackNone) launch_mode<kModeVR, kTrackNone, COUNT>(P, vol, mask, LT, BV, s);
-        else if (track == kTrackShared) launch_mode<kModeVR, kTrackShared, COUNT>(P, vol, mask, LT, BV, s);
-        else launch_mode<kModeVR, kTrackLocal, COUNT>(P, vol, mask, LT, BV, s);
+        if (track == kTrackNone) launch_mode<kModeVR, kTrackNone, COUNT>(P, vol, mask, LT, BV, order, s);
+        else if (track == kTrackShared) launch_mode<kModeVR, kTrackShared, COUNT>(P, vol, mask, LT, BV, order, s);
+        else launch_mode<kModeVR, kTrackLocal, COUNT>(P, vol, mask, LT, BV, order, s);
     } else if (mode == kModeMIP) {
-        launch_mode<kModeMIP, kTrackNone, COUNT>(P, vol, mask, LT, BV, s);
+        launch_mode<kModeMIP, kTrackNone, COUNT>(P, vol, mask, LT, BV, order, s);
     } else {
-        launch_mode<kModeSurface, kTrackNone, COUNT>(P, vol, mask, LT, BV, s);
+        launch_mode<kModeSurface, kTrackNone, COUNT>(P, vol, mask, LT, BV, order, s);
     }
+}
+
+std::vector<int> centre_first_tiles(int W, int H, int xT, int yT) {
+    const int tx = (W + 31) / 32, ty = (H + 7) / 8, n = tx * ty;
+    const double cx = W / 2.0 + xT, cy = H / 2.0 + yT;
+    std::vector<std::pair<double, int>> d((size_t)n);
+    for (int t = 0; t < n; ++t) {
+        const double dx = (t % tx) * 32 + 16 - cx, dy = (t / tx) * 8 + 4 - cy;
+        d[t] = {dx * dx + dy * dy, t};
+    }
+    std::stable_sort(d.begin(), d.end());
+    std::vector<int> h((size_t)n);
+    for (int t = 0; t < n; ++t) h[t] = d[t].second;
+    return h;
+}
+
+// The centre-first tile order of a W x H image whose volume centre projects
+// to (W/2 + xT, H/2 + yT) (core/kernel.cu:161-162 with u = v = 0), cached on
+// the volume.  Tiles are sorted by the distance of their centre to that
+// point; a new table is uploaded on `s` and waited for once, so launches on
+// other streams can share it.
+static int tile_order(VolumeState &v, const RayParams &P, cudaStream_t s, const int **out) {
+    const int key[4] = {P.W, P.H, (int)lrintf(P.xT), (int)lrintf(P.yT)};
+    for (int i = 0; i < v.n_orders; ++i) {
+        const VolumeState::TileOrder &o = v.orders[i];
+        if (o.key[0] == key[0] && o.key[1] == key[1] && o.key[2] == key[2] && o.key[3] == key[3]) {
+            *out = o.d_tiles;
+            return MK_OK;
+        }
+    }
+    const std::vector<int> h = centre_first_tiles(P.W, P.H, key[2], key[3]);
+    const int n = (int)h.size();
+    if (v.n_orders == 16) {                      // drop the oldest
+        MK_CUDA_TRY(cudaStreamSynchronize(s));
+        cudaFree(v.orders[0].d_tiles);
+        for (int i = 1; i < 16; ++i) v.orders[i - 1] = v.orders[i];
+        v.n_orders = 15;
+    }
+    int *dt = nullptr;
+    MK_CUDA_TRY(cudaMalloc(&dt, (size_t)n * sizeof(int)));
+    MK_CUDA_TRY(cudaMemcpyAsync(dt, h.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+    MK_CUDA_TRY(cudaStreamSynchronize(s));
+    VolumeState::TileOrder &o = v.orders[v.n_orders++];
+    for (int k = 0; k < 4; ++k) o.key[k] = key[k];
+    o.d_tiles = dt;
+    *out = dt;
+    return MK_OK;
 }
 
 // Labels that need a per-ray opacity accumulator: present in the mask and
@@ -167,8 +229,11 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     }
     rc = rebuild_brick_maps(&v, s);
     if (rc != MK_OK) return rc;
+    const int *order = nullptr;
+    rc = tile_order(v, P, s, &order);
+    if (rc != MK_OK) return rc;
     launch_raycast<false>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
-                          label_table(&v), brick_view(&v), s);
+                          label_table(&v), brick_view(&v), order, s);
     MK_CUDA_TRY(cudaGetLastError());
     return finish_output(&v, out, bytes, out_on_device, s);
 }
@@ -198,7 +263,7 @@ extern "C" int mk_count_vr_samples(mk_volume vol, const mk_vr_params *params, ui
     rc = rebuild_brick_maps(&v, s);
     if (rc != MK_OK) return rc;
     launch_raycast<true>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
-                         label_table(&v), brick_view(&v), s);
+                         label_table(&v), brick_view(&v), nullptr, s);
     MK_CUDA_TRY(cudaGetLastError());
     unsigned long long h = 0;
     MK_CUDA_TRY(cudaMemcpyAsync(&h, v.d_counter, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -238,7 +303,7 @@ extern "C" int mk_count_vr_footprint(mk_volume vol, const mk_vr_params *params, 
     rc = rebuild_brick_maps(&v, s);
     if (rc == MK_OK) {
         launch_raycast<true>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
-                             label_table(&v), brick_view(&v), s);
+                             label_table(&v), brick_view(&v), nullptr, s);
         k_popcount<<<1184, 256, 0, s>>>(bits, nwords, cnt + 1);
         k_popcount<<<1184, 256, 0, s>>>(bits + nwords, nwords, cnt + 2);
         unsigned long long h[3] = {0, 0, 0};

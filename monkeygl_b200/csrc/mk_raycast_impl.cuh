@@ -8,6 +8,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "mk_internal.h"
 #include "mk_math.h"
 
@@ -533,7 +535,8 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
     s_px[ly][lx * 3 + 2] = (rgb >> 16) & 0xff;
     __syncthreads();
     const int x0 = bx * 32, y0 = by * 8;
-    const bool full = (x0 + 32 <= P.W) && (y0 + 8 <= P.H) && ((P.W & 3) == 0);
+    const bool full = (x0 + 32 <= P.W) && (y0 + 8 <= P.H) && ((P.W & 3) == 0) &&
+                      ((reinterpret_cast<uintptr_t>(P.out) & 3) == 0);   // word stores need an aligned row
     if (full) {
         if (tid < 8 * 24) {
             const int r = tid / 24, w = tid % 24;
@@ -556,5 +559,9 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
 // present in a volume under a table of (alpha, ww, wl) rows.
 int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P);
 int tracking_mode_for(const uint64_t present[2], const float (*params)[3]);
+// Host: the 32x8 tiles of a W x H frame (index by * tiles_x + bx) sorted by
+// the distance of their centre to (W/2 + xT, H/2 + yT), where the volume
+// centre projects: launching them in this order starts the long rays first.
+std::vector<int> centre_first_tiles(int W, int H, int xT, int yT);
 
 }  // namespace mk

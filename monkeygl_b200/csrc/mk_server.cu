@@ -30,10 +30,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -152,6 +154,7 @@ struct Req {
     std::vector<float> luts, params;
     int slot = -1;
     int tiles_x = 0, tiles_total = 0, tiles_issued = 0;
+    std::shared_ptr<const std::vector<int>> order;   // tile order (ray casting: centre first)
     size_t out_bytes = 0;
     bool direct = false;
     bool done = false;
@@ -194,6 +197,7 @@ struct mk_server_s {
     std::map<int, ServerVolume> volumes;
     int next_volume = 1;
     std::map<uint64_t, Req> reqs;
+    std::map<std::array<int, 4>, std::shared_ptr<const std::vector<int>>> orders;   // centre-first tile orders
     std::deque<uint64_t> pending;
     std::vector<uint64_t> active;       // in slots, admission order
     std::deque<Step> inflight;
@@ -352,8 +356,9 @@ int issue_step(mk_server_s *s) {
         while (q.tiles_issued < q.tiles_total && n < s->max_items) {
             const int k = q.tiles_issued++;
             items[n].slot = (unsigned short)q.slot;
-            items[n].tx = (unsigned short)(k % q.tiles_x);
-            items[n].ty = (unsigned short)(k / q.tiles_x);
+            const int t = q.order ? (*q.order)[k] : k;
+            items[n].tx = (unsigned short)(t % q.tiles_x);
+            items[n].ty = (unsigned short)(t / q.tiles_x);
             items[n].pad = 0;
             ++n;
         }
@@ -786,6 +791,14 @@ extern "C" int mk_server_submit(mk_server s, const mk_request *req, uint64_t *ti
         q.tiles_x = (P.W + 31) / 32;
         q.tiles_total = q.tiles_x * ((P.H + 7) / 8);
         q.out_bytes = (size_t)P.W * P.H * (P.rgba ? 4 : 3);
+        const std::array<int, 4> key = {P.W, P.H, (int)lrintf(P.xT), (int)lrintf(P.yT)};
+        auto oit = s->orders.find(key);
+        if (oit == s->orders.end()) {
+            if (s->orders.size() >= 64) s->orders.clear();
+            oit = s->orders.emplace(key, std::make_shared<const std::vector<int>>(
+                                             centre_first_tiles(P.W, P.H, key[2], key[3]))).first;
+        }
+        q.order = oit->second;
     } else {
         set_last_error("mk_server_submit: unknown request kind");
         return MK_ERR_INVALID_ARGUMENT;

@@ -505,6 +505,7 @@ extern "C" int mk_volume_destroy(mk_volume v) {
     cudaFree(st.d_accu);
     cudaFree(st.d_out);
     cudaFree(st.d_counter);
+    for (int i = 0; i < st.n_orders; ++i) cudaFree(st.orders[i].d_tiles);
     if (st.h_pinned) cudaFreeHost(st.h_pinned);
     if (st.stream) cudaStreamDestroy(st.stream);
     cudaGetLastError();
