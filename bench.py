@@ -60,6 +60,7 @@ def parse_args():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="body")
     ap.add_argument("--size", type=int, default=1024)
     ap.add_argument("--suite", action="store_true")
+    ap.add_argument("--suite-only", default="", help="comma list of suite groups: vr,mpr,cpr,dvr (default all)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (monkeygl_b200.serve_bench)")
     ap.add_argument("--serve-requests", type=int, default=10000)
     ap.add_argument("--serve-rate", type=float, default=200.0)

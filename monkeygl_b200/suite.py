@@ -248,13 +248,19 @@ def main(args=None, ref=None):
     torch.cuda.init()
     ctx = {"stream": torch.cuda.Stream(), "flush": torch.empty(256 << 20, dtype=torch.uint8, device="cuda"),
            "ref": ref}
+    only = {g for g in (getattr(args, "suite_only", "") or "").split(",") if g}
+    want = lambda g: not only or g in only
     rows = []
-    rows += vr_rows("cardiac", 0.4, (0, 1), ctx)
-    rows += vr_rows("body", 0.4, (0,), ctx)
-    rows += vr_rows("body", 0.8, (0,), ctx)
-    rows += mpr_rows(ctx)
-    rows += cpr_rows(ctx)
-    rows += dvr_rows(ctx)
+    if want("vr"):
+        rows += vr_rows("cardiac", 0.4, (0, 1), ctx)
+        rows += vr_rows("body", 0.4, (0,), ctx)
+        rows += vr_rows("body", 0.8, (0,), ctx)
+    if want("mpr"):
+        rows += mpr_rows(ctx)
+    if want("cpr"):
+        rows += cpr_rows(ctx)
+    if want("dvr"):
+        rows += dvr_rows(ctx)
     for r in rows:
         print(json.dumps(r), flush=True)
     keys = ["row", "image", "ms", "e2e_ms", "ref_kernel_ms", "ref_call_ms", "speedup_kernel", "speedup_e2e",
