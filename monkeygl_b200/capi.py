@@ -34,6 +34,7 @@ MPR_AVERAGE, MPR_MIP, MPR_MINIP = 0, 1, 2
 SAMPLE_LINEAR, SAMPLE_NEAREST = 0, 1
 PIXEL_RGB8, PIXEL_RGBA8 = 0, 1
 VR_NO_SKIP = 0x1
+VR_NO_COOP = 0x2
 
 
 class MonkeyGLError(RuntimeError):

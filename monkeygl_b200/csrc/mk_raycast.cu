@@ -57,6 +57,7 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
                                                  BrickView BV, const int *__restrict__ order) {
     __shared__ LabelSmem S;
     __shared__ float s_acc[TRACK == kTrackShared ? kMaxTrackedLabels : 1][256];
+    __shared__ CoopSample s_coop[MODE == kModeVR && !COUNT ? 256 : 1];
     __shared__ uint8_t s_px[8][32 * 3];
     __shared__ unsigned long long s_count;
     load_label_smem(S, LT, TRACK);
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
         bx = t % tx;
         by = t / tx;
     }
-    raycast_tile<MODE, TRACK, COUNT>(P, vol, mask, S, BV, s_acc, s_px, &s_count, bx, by);
+    raycast_tile<MODE, TRACK, COUNT>(P, vol, mask, S, BV, s_acc, s_coop, s_px, &s_count, bx, by);
 }
 
 template <int MODE, int TRACK, bool COUNT>
@@ -196,6 +197,7 @@ int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P) {
     P.accu_len = v.accu_len;
     P.rgba = (p->pixel_format == MK_PIXEL_RGBA8) ? 1 : 0;
     P.skip = (p->flags & MK_VR_NO_SKIP) ? 0 : 1;
+    P.coop_rays = (p->flags & MK_VR_NO_COOP) ? 0 : kCoopRaysDefault;
     P.out = nullptr;
     P.counter = nullptr;
     P.vox_bits = nullptr;

@@ -35,6 +35,7 @@ struct RayParams {
     int accu_len;
     int rgba;                    // 1 = 4 bytes per pixel
     int skip;
+    int coop_rays;               // VR: a warp with at most this many rays left marches them cooperatively
     uint8_t *out;
     unsigned long long *counter; // sample counting mode
     uint32_t *vox_bits;          // counting mode: voxels inside trilinear footprints (may be null)
@@ -135,23 +136,58 @@ __device__ __forceinline__ int brick_index(const RayParams &P, const BrickView &
     return ((iz >> kBrickShift) * BV.nby + (iy >> kBrickShift)) * BV.nbx + (ix >> kBrickShift);
 }
 
+// Per-step displacement of a ray in voxel units (dv) and its reciprocal
+// (rdv, 0 where the ray is parallel to an axis), for runs inside empty
+// bricks.
+struct StepVec {
+    float3 dv;
+    float3 rdv;
+};
+
+__device__ __forceinline__ StepVec step_vec(const RayParams &P) {
+    StepVec S;
+    const float ds = P.step1 * P.scale;
+    S.dv.x = P.M[1] * P.mls[0] * ds * P.fdim[0];
+    S.dv.y = P.M[4] * P.mls[1] * ds * P.fdim[1];
+    S.dv.z = P.M[7] * P.mls[2] * ds * P.fdim[2];
+    if (P.invertZ) S.dv.z = -S.dv.z;
+    S.rdv.x = fabsf(S.dv.x) > 1e-6f ? 1.0f / S.dv.x : 0.0f;
+    S.rdv.y = fabsf(S.dv.y) > 1e-6f ? 1.0f / S.dv.y : 0.0f;
+    S.rdv.z = fabsf(S.dv.z) > 1e-6f ? 1.0f / S.dv.z : 0.0f;
+    return S;
+}
+
 // Number of further coarse steps that stay inside brick (bx,by,bz) with a
-// 0.05-voxel margin, capped at 64.  Position p is in voxel units.
-__device__ __forceinline__ int steps_in_brick(const float3 &pv, const float3 &dv, int ix, int iy,
-                                              int iz) {
+// 0.05-voxel margin, capped at 64.  Position p is in voxel units.  Any
+// count that keeps those samples inside the brick is valid (they are all
+// skippable); the margin covers the rounding of the linear model.
+__device__ __forceinline__ int steps_in_brick(const float3 &pv, const StepVec &sv, int ix, int iy, int iz) {
     float t = 64.0f;
     const float e = 0.05f;
     const float lo[3] = {(float)((ix >> kBrickShift) << kBrickShift),
                          (float)((iy >> kBrickShift) << kBrickShift),
                          (float)((iz >> kBrickShift) << kBrickShift)};
     const float pp[3] = {pv.x, pv.y, pv.z};
-    const float dd[3] = {dv.x, dv.y, dv.z};
+    const float rd[3] = {sv.rdv.x, sv.rdv.y, sv.rdv.z};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        if (dd[k] > 1e-6f) t = fminf(t, (lo[k] + kBrick - e - pp[k]) / dd[k]);
-        else if (dd[k] < -1e-6f) t = fminf(t, (pp[k] - lo[k] - e) / -dd[k]);
+        if (rd[k] > 0.0f) t = fminf(t, (lo[k] + kBrick - e - pp[k]) * rd[k]);
+        else if (rd[k] < 0.0f) t = fminf(t, (pp[k] - lo[k] - e) * -rd[k]);
     }
     return t > 0.0f ? (int)t : 0;
+}
+
+// Advance accuLength by n coarse steps: n float additions of L1, as
+// MonkeyGL's loop makes them.  While a ray has never refined its step it
+// stays on the schedule table (a == accu[lat]), whose entry lat + n holds
+// the same sum; lat < 0 once the ray has left it.
+__device__ __forceinline__ void advance_coarse(const RayParams &P, float &a, int &lat, float step, int n) {
+    if (lat >= 0) {
+        lat = min(lat + n, P.accu_len - 1);
+        a = P.accu[lat];
+    } else {
+        for (; n > 0; --n) a += step;
+    }
 }
 
 // Counting mode: mark the eight texels of a trilinear fetch at normalized
@@ -193,13 +229,31 @@ __device__ inline void mark_label(const RayParams &P, int ix, int iy, int iz) {
     atomicOr(&P.lab_bits[idx >> 5], 1u << (idx & 31));
 }
 
-// Central-difference normal and headlight shading (core/kernel.cu:49-81).
-__device__ __forceinline__ float4 shade(float4 sum, float alphaAcc, cudaTextureObject_t vol,
-                                        float3 pos, float4 col, float3 L, const RayParams &P) {
+// Central-difference normal and headlight shading (core/kernel.cu:49-81):
+// the shaded colour of a sample, before it is weighted by the remaining
+// transparency.  It depends only on the sample, not on the ray's state.
+// The six central-difference taps (core/kernel.cu:61-63): +x, -x, +y, -y,
+// +z, -z, one spacing voxel away.
+struct GradTaps {
+    float xp, xm, yp, ym, zp, zm;
+};
+
+__device__ __forceinline__ GradTaps fetch_taps(cudaTextureObject_t vol, float3 pos, const RayParams &P) {
+    GradTaps g;
+    g.xp = tex3D<float>(vol, pos.x + P.sv[0], pos.y, pos.z);
+    g.xm = tex3D<float>(vol, pos.x - P.sv[0], pos.y, pos.z);
+    g.yp = tex3D<float>(vol, pos.x, pos.y + P.sv[1], pos.z);
+    g.ym = tex3D<float>(vol, pos.x, pos.y - P.sv[1], pos.z);
+    g.zp = tex3D<float>(vol, pos.x, pos.y, pos.z + P.sv[2]);
+    g.zm = tex3D<float>(vol, pos.x, pos.y, pos.z - P.sv[2]);
+    return g;
+}
+
+__device__ __forceinline__ float4 shade_taps(const GradTaps &g, float4 col, float3 L, const RayParams &P) {
     float3 N;
-    N.x = tex3D<float>(vol, pos.x + P.sv[0], pos.y, pos.z) - tex3D<float>(vol, pos.x - P.sv[0], pos.y, pos.z);
-    N.y = tex3D<float>(vol, pos.x, pos.y + P.sv[1], pos.z) - tex3D<float>(vol, pos.x, pos.y - P.sv[1], pos.z);
-    N.z = tex3D<float>(vol, pos.x, pos.y, pos.z + P.sv[2]) - tex3D<float>(vol, pos.x, pos.y, pos.z - P.sv[2]);
+    N.x = g.xp - g.xm;
+    N.y = g.yp - g.ym;
+    N.z = g.zp - g.zm;
     if (P.invertZ) N.z = -N.z;
     const float inv = rsqrtf(N.x * N.x + N.y * N.y + N.z * N.z);
     N.x = N.x * inv;
@@ -216,9 +270,24 @@ __device__ __forceinline__ float4 shade(float4 sum, float alphaAcc, cudaTextureO
     clr.y += t4.y;
     clr.z += t4.z;
     clr.w += t4.w;
-    diffuse = (1.0f - alphaAcc) * col.w;
-    return make_float4(sum.x + diffuse * clr.x, sum.y + diffuse * clr.y, sum.z + diffuse * clr.z,
-                       sum.w + diffuse * clr.w);
+    return clr;
+}
+
+// sum + (1 - alphaAcc) * alpha * clr, the return value of tracing()
+// (core/kernel.cu:78-80).
+__device__ __forceinline__ float4 composite(float4 sum, float alphaAcc, float alpha, float4 clr) {
+    const float w = (1.0f - alphaAcc) * alpha;
+    return make_float4(sum.x + w * clr.x, sum.y + w * clr.y, sum.z + w * clr.z, sum.w + w * clr.w);
+}
+
+__device__ __forceinline__ float4 shade_color(cudaTextureObject_t vol, float3 pos, float4 col, float3 L,
+                                              const RayParams &P) {
+    return shade_taps(fetch_taps(vol, pos, P), col, L, P);
+}
+
+__device__ __forceinline__ float4 shade(float4 sum, float alphaAcc, cudaTextureObject_t vol,
+                                        float3 pos, float4 col, float3 L, const RayParams &P) {
+    return composite(sum, alphaAcc, col.w, shade_color(vol, pos, col, L, P));
 }
 
 // rgbaFloatToInt (core/kernel.cu:40-47): saturate, scale by 255, truncate.
@@ -253,6 +322,379 @@ __device__ __forceinline__ void load_label_smem(LabelSmem &S, const LabelTable &
     }
 }
 
+// ---------------------------------------------------------------------------
+// VR march of one warp's rays with a cooperative tail.
+//
+// A ray is a chain of dependent steps (sample position, texture fetch, LUT
+// fetch, opacity correction, shading fetches), so a warp whose last few rays
+// are long runs at the latency of that chain with most lanes idle; on a
+// 1024^2 frame one such warp can take three times as long as the average SM
+// is busy.  When at most P.coop_rays rays of a warp are left, its 32 lanes
+// are split into groups of G = 32/rays (a power of two) and each group takes
+// one ray: lane j of a group evaluates the sample j steps ahead at the
+// current step size (position, label, value, LUT, opacity correction and,
+// for alpha > 0.0005, the shaded colour), all in parallel, and then every
+// lane of the group walks MonkeyGL's schedule over those samples in order
+// (refinement, coarsening, empty-brick runs, opacity caps, compositing,
+// termination).  The walk stops at the first sample whose successor was not
+// evaluated at the right place (the step changed) and the next round starts
+// there.  A sample depends only on its accuLength, and the walk applies the
+// same float operations in the same order as the one-lane march, so the
+// image is unchanged.
+
+// Result of evaluating one sample.  meta: bits 0-3 kCoop* flags, 4-11 label,
+// 12-19 further steps of an empty-brick run.
+struct __align__(16) CoopSample {
+    float4 clr;      // shaded colour (alpha > 0.0005)
+    float4 res;      // final colour of the ray whose pixel is this lane's
+    float alpha;     // opacity-corrected alpha at the round's step
+    int meta;
+    int pad[2];
+};
+constexpr int kCoopEnd = 1;        // past the end of the ray (a >= limit or a > a_stop)
+constexpr int kCoopOutside = 2;    // outside the VOI: no fetch
+constexpr int kCoopEmpty = 4;      // in a brick with its visibility bit clear (step L1)
+constexpr int kCoopFetched = 8;    // label, value and LUT fetched
+constexpr int kCoopRaysDefault = 16;
+
+struct VrRay {
+    float u, v, a, a_stop, step, aPre, A;
+    float4 sum;
+    int lat;         // index of a in the schedule table while the step was never refined, else -1
+    bool done;
+};
+
+template <int TRACK>
+__device__ __forceinline__ bool vr_cap_ok(const LabelSmem &S, const float (*s_acc)[256], const float *accLocal,
+                                          int label, int owner) {
+    const signed char sl = S.slot[label];
+    if (TRACK == kTrackLocal) return (sl != -2) && accLocal[label] < S.alpha[label];
+    if (sl == -2) return false;
+    if (sl == -1) return true;
+    return s_acc[sl][owner] < S.alpha[label];
+}
+
+template <int TRACK>
+__device__ __forceinline__ void vr_cap_add(const LabelSmem &S, float (*s_acc)[256], float *accLocal, int label,
+                                           int owner, float A, float alpha) {
+    const signed char sl = S.slot[label];
+    if (TRACK == kTrackLocal) accLocal[label] += (1.0f - A) * alpha;
+    else if (TRACK == kTrackShared && sl >= 0) s_acc[sl][owner] += (1.0f - A) * alpha;
+}
+
+// The cooperative tail: every lane of the warp calls it with the warp's
+// mask of unfinished rays `act`; on return each lane of `act` holds its
+// ray's final colour in R.sum.  Groups widen as rays finish: whenever the
+// unfinished rays fit into groups twice as large, their states move to new
+// groups, so a warp's last ray is marched by all 32 lanes.
+template <int TRACK>
+__device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+                             const LabelSmem &S, const BrickView &BV, float (*s_acc)[256], CoopSample *ws,
+                             unsigned act, VrRay &R, const StepVec &dv, float3 L) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const float L1 = P.step1, L4 = L1 / 4.0f, L8 = L1 / 8.0f;
+    VrRay Q = R;            // the ray this lane works on; initially its own
+    int owner = lane;       // lane of Q's pixel (and of its opacity caps)
+    unsigned cur = act;     // lanes whose Q is an unfinished ray, to be grouped
+    while (cur) {
+        const int nrays = __popc(cur);
+        int G = 32;
+        while (G * nrays > 32) G >>= 1;
+        const int g = lane / G, j = lane - g * G;
+        const bool member = g < nrays;
+        int src = lane;     // holder of ray g: the g-th set bit of cur
+        if (member) {
+            unsigned m = cur;
+            for (int i = 0; i < g; ++i) m &= m - 1u;
+            src = __ffs(m) - 1;
+        }
+        {
+            VrRay T;
+            T.u = __shfl_sync(FULL, Q.u, src);
+            T.v = __shfl_sync(FULL, Q.v, src);
+            T.a = __shfl_sync(FULL, Q.a, src);
+            T.a_stop = __shfl_sync(FULL, Q.a_stop, src);
+            T.step = __shfl_sync(FULL, Q.step, src);
+            T.aPre = __shfl_sync(FULL, Q.aPre, src);
+            T.A = __shfl_sync(FULL, Q.A, src);
+            T.sum.x = __shfl_sync(FULL, Q.sum.x, src);
+            T.sum.y = __shfl_sync(FULL, Q.sum.y, src);
+            T.sum.z = __shfl_sync(FULL, Q.sum.z, src);
+            T.sum.w = __shfl_sync(FULL, Q.sum.w, src);
+            T.lat = __shfl_sync(FULL, Q.lat, src);
+            owner = __shfl_sync(FULL, owner, src);
+            T.done = !member;
+            Q = T;
+        }
+        const int owner_tid = (threadIdx.x & ~31) | owner;
+        bool reported = false;
+        while (true) {
+            // 1. this lane's sample, j steps ahead
+            float4 clr = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            float alpha_j = 0.0f;
+            int flags = 0, label = 0, nskip = 0;
+            if (!Q.done) {
+                float aj = Q.a;
+                if (Q.lat >= 0) aj = P.accu[min(Q.lat + j, P.accu_len - 1)];
+                else
+                    for (int k = 0; k < j; ++k) aj += Q.step;
+                if (!(aj < P.limit) || aj > Q.a_stop) {
+                    flags = kCoopEnd;
+                } else {
+                    const float3 pos = ray_pos(P, Q.u, Q.v, aj);
+                    const int ix = pos.x * P.fdim[0];
+                    const int iy = pos.y * P.fdim[1];
+                    const int iz = pos.z * P.fdim[2];
+                    if (outside_voi(P, ix, iy, iz)) {
+                        flags = kCoopOutside;
+                    } else {
+                        bool empty = false;
+                        if (P.skip && Q.step == L1) {
+                            const int b = brick_index(P, BV, ix, iy, iz);
+                            empty = !((BV.visible_bits[b >> 5] >> (b & 31)) & 1u);
+                            if (empty) {
+                                const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1], pos.z * P.fdim[2]);
+                                nskip = steps_in_brick(pv, dv, ix, iy, iz);
+                                flags |= kCoopEmpty;
+                            }
+                        }
+                        // an empty-brick sample is fetched only where the walk may not skip it
+                        if (!empty || (j == 0 && !(Q.aPre <= 0.001f))) {
+                            label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
+                            float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
+                            temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
+                            if (temp > 1) temp = 1;
+                            const cudaTextureObject_t tf = S.tf[label];
+                            const float4 col = tf ? tex1D<float4>(tf, temp) : make_float4(0.f, 0.f, 0.f, 0.f);
+                            float alpha = col.w;
+                            if (Q.step == L4) alpha = 1 - powf(1 - alpha, 0.25f);
+                            else if (Q.step == L8) alpha = 1 - powf(1 - alpha, 0.125f);
+                            alpha_j = alpha;
+                            if (alpha > 0.0005f)
+                                clr = shade_color(vol, pos, make_float4(col.x, col.y, col.z, alpha), L, P);
+                            flags |= kCoopFetched;
+                        }
+                    }
+                }
+            }
+            ws[lane].clr = clr;
+            ws[lane].alpha = alpha_j;
+            ws[lane].meta = flags | (label << 4) | (nskip << 12);
+            __syncwarp();
+
+            // 2. MonkeyGL's schedule over the group's samples, in order
+            if (!Q.done) {
+                int k = 0;
+                while (k < G) {
+                    const int meta = ws[g * G + k].meta;
+                    const int f = meta & 15;
+                    if (f & kCoopEnd) {
+                        Q.done = true;
+                        break;
+                    }
+                    if (f & kCoopOutside) {
+                        Q.a += Q.step;
+                        if (Q.lat >= 0) ++Q.lat;
+                        ++k;
+                        continue;
+                    }
+                    if ((f & kCoopEmpty) && P.skip && Q.step == L1 && Q.aPre <= 0.001f) {
+                        const int n = 1 + ((meta >> 12) & 255);
+                        Q.aPre = 0.0f;
+                        advance_coarse(P, Q.a, Q.lat, Q.step, n);
+                        k += n;
+                        continue;
+                    }
+                    if (!(f & kCoopFetched)) break;   // evaluate it in the next round
+                    const float alpha = ws[g * G + k].alpha;
+                    bool last = false;
+                    if (Q.a > 0.0f) {
+                        if ((alpha > Q.aPre ? alpha : Q.aPre) > 0.001f) {
+                            if (Q.step == L1) {
+                                Q.a -= (L1 - L4);
+                                Q.step = L4;
+                                Q.lat = -1;
+                                break;
+                            } else if (Q.step == L4) {
+                                Q.a -= (L4 - L8);
+                                Q.step = L8;
+                                break;
+                            }
+                        } else {
+                            const float ns = (Q.step == L8) ? L4 : L1;
+                            last = ns != Q.step;
+                            Q.step = ns;
+                        }
+                    } else {
+                        last = true;
+                    }
+                    Q.aPre = alpha;
+                    Q.a += Q.step;
+                    if (Q.lat >= 0) ++Q.lat;
+                    if (alpha > 0.0005f) {
+                        const int lab = (meta >> 4) & 255;
+                        if (vr_cap_ok<TRACK>(S, s_acc, nullptr, lab, owner_tid)) {
+                            Q.sum = composite(Q.sum, Q.A, alpha, ws[g * G + k].clr);
+                            vr_cap_add<TRACK>(S, s_acc, nullptr, lab, owner_tid, Q.A, alpha);
+                            Q.A += (1.0f - Q.A) * alpha;
+                        }
+                    }
+                    if (Q.A > 0.995f) {
+                        Q.done = true;
+                        break;
+                    }
+                    if (last) break;
+                    ++k;
+                }
+            }
+            if (member && Q.done && !reported) {
+                if (j == 0) ws[owner].res = Q.sum;
+                reported = true;
+            }
+            __syncwarp();
+            const unsigned live = __ballot_sync(FULL, member && j == 0 && !Q.done);
+            if (live == 0u) {
+                cur = 0u;
+                break;
+            }
+            if (G < 32 && __popc(live) * 2 * G <= 32) {
+                cur = live;          // regroup the unfinished rays into wider groups
+                break;
+            }
+        }
+    }
+    __syncwarp();
+    if ((act >> lane) & 1u) R.sum = ws[lane].res;
+    __syncwarp();
+}
+
+// MonkeyGL's d_render march (core/kernel.cu:156-256) for the ray of this
+// lane, called by every lane of the warp; returns the composited colour
+// (the background where nothing composited).
+template <int TRACK>
+__device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+                                           const LabelSmem &S, const BrickView &BV, float (*s_acc)[256],
+                                           CoopSample *ws, bool active, int x, int y) {
+    const int tid = threadIdx.x;
+    VrRay R;
+    R.u = R.v = R.a = R.a_stop = 0.0f;
+    R.step = P.step1;
+    R.aPre = 0.0f;
+    R.A = 0.0f;
+    R.sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    R.lat = -1;
+    R.done = true;
+    if (active) {
+        R.u = 1.0f * (x - P.W / 2.0f - P.xT) / P.H;
+        R.v = 1.0f * (y - P.H / 2.0f - P.yT) / P.H;
+        float a0, a1;
+        if (ray_interval(P, R.u, R.v, a0, a1)) {
+            int k0 = accu_lower(P, a0);
+            k0 = k0 > 0 ? k0 - 1 : 0;
+            R.a = P.accu[k0];
+            R.lat = k0;
+            R.a_stop = a1;
+            R.done = false;
+        }
+    }
+    const StepVec dv = step_vec(P);
+    float3 L;
+    {
+        // normalize(mul(M, (0,1,0))) (core/kernel.cu:166-167)
+        float lx_ = dot3(0.0f, 1.0f, 0.0f, P.M[0], P.M[1], P.M[2]);
+        float ly_ = dot3(0.0f, 1.0f, 0.0f, P.M[3], P.M[4], P.M[5]);
+        float lz_ = dot3(0.0f, 1.0f, 0.0f, P.M[6], P.M[7], P.M[8]);
+        const float inv = rsqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_);
+        L = make_float3(lx_ * inv, ly_ * inv, lz_ * inv);
+    }
+    const float L1 = P.step1;
+    const float L4 = L1 / 4.0f;
+    const float L8 = L1 / 8.0f;
+    float accLocal[TRACK == kTrackLocal ? MK_MAX_LABELS : 1];
+    if (TRACK == kTrackShared) {
+        for (int i = 0; i < kMaxTrackedLabels; ++i) s_acc[i][tid] = 0.0f;
+    } else if (TRACK == kTrackLocal) {
+        for (int i = 0; i < MK_MAX_LABELS; ++i) accLocal[i] = 0.0f;
+    }
+    while (true) {
+        const unsigned act = __ballot_sync(0xffffffffu, !R.done);
+        if (act == 0u) break;
+        if (TRACK != kTrackLocal && __popc(act) <= P.coop_rays) {
+            vr_coop_tail<TRACK>(P, vol, mask, S, BV, s_acc, ws + (tid & ~31), act, R, dv, L);
+            break;
+        }
+        if (R.done) continue;
+        // one step of the schedule: a sample outside the VOI, a run of
+        // samples in an empty brick, or a fetched sample (lanes that take
+        // different ones diverge only within this iteration)
+        do {
+            if (!(R.a < P.limit) || R.a > R.a_stop) {
+                R.done = true;
+                break;
+            }
+            const float3 pos = ray_pos(P, R.u, R.v, R.a);
+            const int ix = pos.x * P.fdim[0];
+            const int iy = pos.y * P.fdim[1];
+            const int iz = pos.z * P.fdim[2];
+            if (outside_voi(P, ix, iy, iz)) {
+                R.a += R.step;
+                if (R.lat >= 0) ++R.lat;
+                break;
+            }
+            if (P.skip && R.step == L1 && R.aPre <= 0.001f) {
+                const int b = brick_index(P, BV, ix, iy, iz);
+                if (!((BV.visible_bits[b >> 5] >> (b & 31)) & 1u)) {
+                    R.aPre = 0.0f;
+                    const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1], pos.z * P.fdim[2]);
+                    advance_coarse(P, R.a, R.lat, R.step, 1 + steps_in_brick(pv, dv, ix, iy, iz));
+                    break;
+                }
+            }
+            const int label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
+            float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
+            temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
+            if (temp > 1) temp = 1;
+            const cudaTextureObject_t tf = S.tf[label];
+            float4 col = tf ? tex1D<float4>(tf, temp) : make_float4(0.f, 0.f, 0.f, 0.f);
+            float alpha = col.w;
+            // getNextStep (core/kernel.cu:84-125)
+            if (R.step == L4) alpha = 1 - powf(1 - alpha, 0.25f);
+            else if (R.step == L8) alpha = 1 - powf(1 - alpha, 0.125f);
+            if (R.a > 0.0f) {
+                if ((alpha > R.aPre ? alpha : R.aPre) > 0.001f) {
+                    if (R.step == L1) {
+                        R.a -= (L1 - L4);
+                        R.step = L4;
+                        R.lat = -1;
+                        break;
+                    } else if (R.step == L4) {
+                        R.a -= (L4 - L8);
+                        R.step = L8;
+                        break;
+                    }
+                } else {
+                    if (R.step == L8) R.step = L4;
+                    else R.step = L1;
+                }
+            }
+            R.aPre = alpha;
+            R.a += R.step;
+            if (R.lat >= 0) ++R.lat;
+            col.w = alpha;
+            if (col.w > 0.0005f && vr_cap_ok<TRACK>(S, s_acc, accLocal, label, tid)) {
+                R.sum = composite(R.sum, R.A, col.w, shade_color(vol, pos, col, L, P));
+                vr_cap_add<TRACK>(S, s_acc, accLocal, label, tid, R.A, col.w);
+                R.A += (1.0f - R.A) * col.w;
+            }
+            if (R.A > 0.995f) R.done = true;
+        } while (0);
+    }
+    float4 sum = R.sum;
+    if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;
+    return sum;
+}
+
 // One 32x8 pixel tile (bx, by) of a frame, by a 256-thread block: eight 8x4
 // warp tiles.  s_acc holds the tracked opacity accumulators (kTrackShared),
 // s_px the tile's RGB bytes, s_count the counting-mode total (zeroed by the
@@ -260,8 +702,8 @@ __device__ __forceinline__ void load_label_smem(LabelSmem &S, const LabelTable &
 template <int MODE, int TRACK, bool COUNT>
 __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
                                              const LabelSmem &S, const BrickView &BV, float (*s_acc)[256],
-                                             uint8_t (*s_px)[32 * 3], unsigned long long *s_count, int bx,
-                                             int by) {
+                                             CoopSample *s_coop, uint8_t (*s_px)[32 * 3],
+                                             unsigned long long *s_count, int bx, int by) {
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int lx = (warp & 3) * 8 + (lane & 7);
@@ -274,7 +716,9 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
     unsigned long long nsamples = 0;
     float A = 0.0f;   // alphaAcc (VR, MIP max, SURFACE last N.L)
 
-    if (active) {
+    if (MODE == kModeVR && !COUNT) {
+        sum = vr_march<TRACK>(P, vol, mask, S, BV, s_acc, s_coop, active, x, y);
+    } else if (active) {
         const float u = 1.0f * (x - P.W / 2.0f - P.xT) / P.H;
         const float v = 1.0f * (y - P.H / 2.0f - P.yT) / P.H;
         float a0, a1;
@@ -286,25 +730,11 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
             const float a_stop = a1;
 
             // per-step displacement in voxel units, for runs inside empty bricks
-            float3 dv;
-            {
-                const float ds = P.step1 * P.scale;
-                dv.x = P.M[1] * P.mls[0] * ds * P.fdim[0];
-                dv.y = P.M[4] * P.mls[1] * ds * P.fdim[1];
-                dv.z = P.M[7] * P.mls[2] * ds * P.fdim[2];
-                if (P.invertZ) dv.z = -dv.z;
-            }
+            const StepVec dv = step_vec(P);
 
             if (MODE == kModeVR) {
-                float3 L;
-                {
-                    // normalize(mul(M, (0,1,0))) (core/kernel.cu:166-167)
-                    float lx_ = dot3(0.0f, 1.0f, 0.0f, P.M[0], P.M[1], P.M[2]);
-                    float ly_ = dot3(0.0f, 1.0f, 0.0f, P.M[3], P.M[4], P.M[5]);
-                    float lz_ = dot3(0.0f, 1.0f, 0.0f, P.M[6], P.M[7], P.M[8]);
-                    const float inv = rsqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_);
-                    L = make_float3(lx_ * inv, ly_ * inv, lz_ * inv);
-                }
+                // counting pass over MonkeyGL's schedule: every sample is
+                // fetched (no skipping); rendering goes through vr_march
                 const float L1 = P.step1;
                 const float L4 = L1 / 4.0f;
                 const float L8 = L1 / 8.0f;
@@ -326,23 +756,9 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                         a += step;
                         continue;
                     }
-                    if (!COUNT && P.skip && step == L1 && aPre <= 0.001f) {
-                        const int b = brick_index(P, BV, ix, iy, iz);
-                        if (!((BV.visible_bits[b >> 5] >> (b & 31)) & 1u)) {
-                            aPre = 0.0f;
-                            a += step;
-                            const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1],
-                                                          pos.z * P.fdim[2]);
-                            int n = steps_in_brick(pv, dv, ix, iy, iz);
-                            for (; n > 0; --n) a += step;
-                            continue;
-                        }
-                    }
-                    if (COUNT) {
-                        ++nsamples;
-                        mark_footprint(P, pos.x, pos.y, pos.z);
-                        if (mask) mark_label(P, ix, iy, iz);
-                    }
+                    ++nsamples;
+                    mark_footprint(P, pos.x, pos.y, pos.z);
+                    if (mask) mark_label(P, ix, iy, iz);
                     const int label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
                     float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
                     temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
@@ -372,35 +788,11 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                     aPre = alpha;
                     a += step;
                     col.w = alpha;
-                    if (COUNT) {
-                        // counting pass: composite decisions still matter for termination
-                        if (col.w > 0.0005f) {
-                            const signed char sl = S.slot[label];
-                            bool ok;
-                            if (TRACK == kTrackLocal) ok = (sl != -2) && accLocal[label] < S.alpha[label];
-                            else if (sl == -2) ok = false;
-                            else if (sl == -1) ok = true;
-                            else ok = s_acc[sl][tid] < S.alpha[label];
-                            if (ok) {
-                                mark_gradient(P, pos);
-                                if (TRACK == kTrackLocal) accLocal[label] += (1.0f - A) * col.w;
-                                else if (TRACK == kTrackShared && sl >= 0) s_acc[sl][tid] += (1.0f - A) * col.w;
-                                A += (1.0f - A) * col.w;
-                            }
-                        }
-                    } else if (col.w > 0.0005f) {
-                        const signed char sl = S.slot[label];
-                        bool ok;
-                        if (TRACK == kTrackLocal) ok = (sl != -2) && accLocal[label] < S.alpha[label];
-                        else if (sl == -2) ok = false;
-                        else if (sl == -1) ok = true;
-                        else ok = s_acc[sl][tid] < S.alpha[label];
-                        if (ok) {
-                            sum = shade(sum, A, vol, pos, col, L, P);
-                            if (TRACK == kTrackLocal) accLocal[label] += (1.0f - A) * col.w;
-                            else if (TRACK == kTrackShared && sl >= 0) s_acc[sl][tid] += (1.0f - A) * col.w;
-                            A += (1.0f - A) * col.w;
-                        }
+                    // composite decisions still matter for termination
+                    if (col.w > 0.0005f && vr_cap_ok<TRACK>(S, s_acc, accLocal, label, tid)) {
+                        mark_gradient(P, pos);
+                        vr_cap_add<TRACK>(S, s_acc, accLocal, label, tid, A, col.w);
+                        A += (1.0f - A) * col.w;
                     }
                     if (A > 0.995f) break;
                 }

@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(256, 3) k_serve(const SlotDesc *__restrict__ s
     __shared__ RayParams s_rp;
     __shared__ BrickView s_bv;
     __shared__ float s_acc[kMaxTrackedLabels][256];
+    __shared__ CoopSample s_coop[256];
     __shared__ uint8_t s_px[8][32 * 3];
     __shared__ unsigned long long s_count;
     __shared__ int s_item, s_slot;
@@ -104,17 +105,17 @@ __global__ void __launch_bounds__(256, 3) k_serve(const SlotDesc *__restrict__ s
             const cudaTextureObject_t vol = D.vol, mask = D.mask;
             if (mode == kModeVR) {
                 if (track == kTrackNone)
-                    raycast_tile<kModeVR, kTrackNone, false>(s_rp, vol, mask, S, s_bv, s_acc, s_px, &s_count, t.tx, t.ty);
+                    raycast_tile<kModeVR, kTrackNone, false>(s_rp, vol, mask, S, s_bv, s_acc, s_coop, s_px, &s_count, t.tx, t.ty);
                 else if (track == kTrackShared)
-                    raycast_tile<kModeVR, kTrackShared, false>(s_rp, vol, mask, S, s_bv, s_acc, s_px, &s_count, t.tx,
+                    raycast_tile<kModeVR, kTrackShared, false>(s_rp, vol, mask, S, s_bv, s_acc, s_coop, s_px, &s_count, t.tx,
                                                                t.ty);
                 else
-                    raycast_tile<kModeVR, kTrackLocal, false>(s_rp, vol, mask, S, s_bv, s_acc, s_px, &s_count, t.tx,
+                    raycast_tile<kModeVR, kTrackLocal, false>(s_rp, vol, mask, S, s_bv, s_acc, s_coop, s_px, &s_count, t.tx,
                                                               t.ty);
             } else if (mode == kModeMIP) {
-                raycast_tile<kModeMIP, kTrackNone, false>(s_rp, vol, mask, S, s_bv, s_acc, s_px, &s_count, t.tx, t.ty);
+                raycast_tile<kModeMIP, kTrackNone, false>(s_rp, vol, mask, S, s_bv, s_acc, s_coop, s_px, &s_count, t.tx, t.ty);
             } else {
-                raycast_tile<kModeSurface, kTrackNone, false>(s_rp, vol, mask, S, s_bv, s_acc, s_px, &s_count, t.tx,
+                raycast_tile<kModeSurface, kTrackNone, false>(s_rp, vol, mask, S, s_bv, s_acc, s_coop, s_px, &s_count, t.tx,
                                                               t.ty);
             }
         } else {

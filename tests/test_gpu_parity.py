@@ -89,6 +89,8 @@ def test_small_raycast_matches_reference(ref, small, small_vol, rtype, angle):
     assert_image_parity(m, r, f"small type {rtype} {angle}", exact=True)
     p.flags = capi.VR_NO_SKIP
     assert np.array_equal(small_vol.render_vr(p), m), "empty-space skipping changed the image"
+    p.flags = capi.VR_NO_COOP
+    assert np.array_equal(small_vol.render_vr(p), m), "the cooperative tail changed the image"
 
 
 def test_small_camera_variants(ref, small, small_vol):
@@ -178,6 +180,10 @@ def test_multilabel_matches_reference(ref, labelled, bg):
             assert_image_parity(m, r, f"labels bg {bg} type {rtype} {ang}", exact=True)
             p.flags = capi.VR_NO_SKIP
             assert np.array_equal(v.render_vr(p), m)
+            p.flags = capi.VR_NO_COOP
+            assert np.array_equal(v.render_vr(p), m)
+            p.flags = capi.VR_NO_COOP | capi.VR_NO_SKIP
+            assert np.array_equal(v.render_vr(p), m)
     # many capped labels force the local-memory path
     lp2 = lp.copy()
     lp2[:20, 0] = 0.5
@@ -198,6 +204,42 @@ def test_cardiac_frame_matches_reference(ref):
         p = params(w, 40.0, rtype)
         r = ref.render(p.width, p.height, rtype, capi.vr_params_flat(p, w.label_params))
         assert_image_parity(v.render_vr(p), r, f"cardiac type {rtype}", exact=True)
+    v.close()
+
+
+def test_cooperative_tail_matches_reference(ref, labelled):
+    """VR warps finish their last rays with several lanes per ray (lanes
+    evaluate the samples ahead, then walk MonkeyGL's schedule over them).
+    Sparse images -- a small VOI, a zoomed-out camera, thin image strips --
+    leave most warps with few rays from the start, so most samples of these
+    frames go through that path.  Each image must equal MonkeyGL's and the
+    one-lane-per-ray march, with and without empty-space skipping."""
+    w = labelled
+    lp = w.label_params.copy()
+    v = capi.Volume(w.phantom.volume)
+    v.set_mask(w.phantom.labels)
+    for l, lut in w.luts.items():
+        v.set_transfer_function(l, lut)
+    v.set_label_params(lp)
+    load_ref(ref, w)
+    cams = []
+    cam = Camera(); cam.anterior(); cam.zoom(0.35); cam.rotate(25.0, 10.0)
+    cams.append(("zoomed-out", cam, {}, (256, 256)))
+    cam = Camera(); cam.left(); cam.rotate(40.0, -15.0)
+    cams.append(("voi", cam, dict(voi=(30, 50, 20, 60, 40, 90)), (256, 192)))
+    cam = Camera(); cam.anterior(); cam.zoom(2.5); cam.rotate(70.0, 0.0)
+    cams.append(("strip", cam, {}, (509, 3)))
+    cam = Camera(); cam.head(); cam.rotate(-35.0, 20.0)
+    cams.append(("column", cam, dict(invert_z=True), (5, 300)))
+    for name, cam, kw, (W, H) in cams:
+        for flags in (0, capi.VR_NO_SKIP):
+            p = capi.vr_params(W, H, 0, cam, w.dims, w.spacing, **kw)
+            p.flags = flags
+            r = ref.render(W, H, 0, capi.vr_params_flat(p, lp))
+            m = v.render_vr(p)
+            assert_image_parity(m, r, f"coop {name} flags {flags}", exact=True)
+            p.flags = flags | capi.VR_NO_COOP
+            assert np.array_equal(v.render_vr(p), m), f"coop {name}: differs from the one-lane march"
     v.close()
 
 
