@@ -312,6 +312,34 @@ int mk_render_cpr_noalloc(mk_volume vol, int width, int height, const double *po
 int mk_volume_synchronize(mk_volume vol, void *stream);
 
 /* ------------------------------------------------------------------ */
+/* VR image overlays (host)                                            */
+/* ------------------------------------------------------------------ */
+
+/* The orientation mesh: a binary STL, centred, scaled by the larger of its
+ * x and z extents and mirrored in z, as MonkeyGL's MarchingCube loads
+ * ./resources/human.stl (core/MarchingCube.cpp:305-354).  MK_ERR_INVALID_ARGUMENT
+ * for a missing, short or truncated file. */
+typedef struct mk_mesh_s *mk_mesh;
+int mk_mesh_load_stl(const char *path, mk_mesh *out);
+int mk_mesh_destroy(mk_mesh mesh);
+int mk_mesh_facet_count(mk_mesh mesh);
+
+/* VRImageLayer::MergeOrientationBox (core/VRImageLayer.cpp:99-194): the mesh,
+ * turned by the camera's 3x3 rotation (RenderInfo's rotate matrix, row-major),
+ * flat-shaded and z-buffered on a 512x512 raster, drawn every 8th pixel into
+ * the bottom-right 64x64 pixels of an RGB8 image (colour (0.902, 0.902,
+ * 0.302) * shade + 0.05).  Nothing is drawn when either side is <= 64.
+ * Host memory; pixels equal MonkeyGL's. */
+int mk_merge_orientation_box(mk_mesh mesh, const float rotate[9], uint8_t *rgb, int width, int height);
+
+/* Methods::DrawLineInImage24Bit (core/Methods.cpp:183-200): a line of
+ * `line_width` parallel strokes, one dot every half pixel, in colour
+ * (r, g, b) in [0, 1]; the CPR line layer draws the projected CPR path with
+ * it (core/CPRLineLayer.cpp:40-65).  Host memory. */
+int mk_draw_line_rgb(uint8_t *rgb, int width, int height, float x0, float y0, float x1, float y1,
+                     int line_width, const float color[3]);
+
+/* ------------------------------------------------------------------ */
 /* Serving: continuous batching of VR/MIP/MPR requests                 */
 /* ------------------------------------------------------------------ */
 

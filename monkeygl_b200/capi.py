@@ -133,6 +133,12 @@ _SIGS = {
                                      C.c_void_p, C.c_int, C.c_void_p]),
     "mk_render_cpr": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                 C.c_void_p, C.c_int, C.c_void_p]),
+    "mk_mesh_load_stl": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "mk_mesh_destroy": (C.c_int, [C.c_void_p]),
+    "mk_mesh_facet_count": (C.c_int, [C.c_void_p]),
+    "mk_merge_orientation_box": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
+    "mk_draw_line_rgb": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                   C.c_int, C.c_void_p]),
     "mk_render_cpr_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_void_p]),
     "mk_volume_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),

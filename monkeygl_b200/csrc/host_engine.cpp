@@ -256,10 +256,14 @@ Engine::Engine() {
     identity(xf_);
     identity(xfT_);
     identity(kernelMatrix_);
+    // MarchingCube's constructor reads the orientation mesh relative to the
+    // working directory (core/MarchingCube.cpp:298)
+    if (mk_mesh_load_stl("./resources/human.stl", &mesh_) != MK_OK) mesh_ = nullptr;
 }
 
 Engine::~Engine() {
     if (dev_) mk_volume_destroy(dev_);
+    if (mesh_) mk_mesh_destroy(mesh_);
 }
 
 // ---- volume (DataManager.cpp:144-175, VolumeInfo.cpp:78-148) -------------
@@ -1175,6 +1179,10 @@ bool Engine::SyncDevice() {
     return true;
 }
 
+// The VR provider's layers in MonkeyGL's order (core/VRProvider.cpp:30-36):
+// the ray-cast image with the orientation box in its bottom-right corner
+// (core/VRImageLayer.cpp:64-145), then the CPR path as a 1-pixel polyline in
+// the line colour (core/CPRLineLayer.cpp:40-65).
 bool Engine::RenderVR(std::shared_ptr<unsigned char> &out, int &w, int &h) {
     if (!LayerEnabled(LayerTypeImage)) return false;
     mk_vr_params p;
@@ -1182,7 +1190,20 @@ bool Engine::RenderVR(std::shared_ptr<unsigned char> &out, int &w, int &h) {
     w = p.width;
     h = p.height;
     out.reset(new unsigned char[(size_t)w * h * 3], std::default_delete<unsigned char[]>());
-    return mk_render_vr(dev_, &p, out.get(), 0, nullptr) == MK_OK;
+    if (mk_render_vr(dev_, &p, out.get(), 0, nullptr) != MK_OK) return false;
+    if (mesh_) mk_merge_orientation_box(mesh_, rot_, out.get(), w, h);
+    if (LayerEnabled(LayerTypeCPRLine) && cprLine_.size() >= 2) {
+        const float clr[3] = {cprColor_.red, cprColor_.green, cprColor_.blue};
+        float x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+        TransferVoxel2ImageInVR(x0, y0, w, h, cprLine_[0]);
+        for (size_t i = 1; i < cprLine_.size(); ++i) {
+            TransferVoxel2ImageInVR(x1, y1, w, h, cprLine_[i]);
+            mk_draw_line_rgb(out.get(), w, h, x0, y0, x1, y1, 1, clr);
+            x0 = x1;
+            y0 = y1;
+        }
+    }
+    return true;
 }
 
 bool Engine::RenderPlane(std::shared_ptr<short> &out, int &w, int &h, PlaneType t) {

@@ -219,6 +219,10 @@ private:
     std::vector<Annotation> annotations_;
     int planeLabel_ = 0;
 
+    // orientation box mesh (./resources/human.stl at construction, as
+    // MonkeyGL's MarchingCube loads it); null when the file is absent
+    mk_mesh mesh_ = nullptr;
+
     // device
     mk_volume dev_ = nullptr;
     bool tfDirty_ = true, tableDirty_ = true, maskDirty_ = false, volumeDirty_ = false;

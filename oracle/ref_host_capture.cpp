@@ -22,6 +22,7 @@
 #include "DataManager.h"
 #include "Defines.h"
 #include "HelloMonkey.h"
+#include "Methods.h"
 #include "TransferFunction.h"
 
 using namespace MonkeyGL;
@@ -356,4 +357,16 @@ extern "C" int mkrh_tf_lut(const int *rgb_pos, const float *rgba, int n_rgb, con
     if (n > max_len) return -n;
     memcpy(out_rgba, buf.get(), (size_t)n * sizeof(RGBA));
     return n;
+}
+
+// RenderInfo's rotate matrix (the one VRImageLayer::GetMeshPoints turns the
+// orientation mesh with), row-major.
+extern "C" void mkrh_rotate_matrix(float *out) {
+    memcpy(out, DataManager::Instance()->GetRenderInfo().GetRotateMatrix(), 9 * sizeof(float));
+}
+
+// Methods::DrawLineInImage24Bit on an RGB image.
+extern "C" void mkrh_draw_line(unsigned char *img, int w, int h, float x0, float y0, float x1, float y1, int lw,
+                               float r, float g, float b) {
+    Methods::DrawLineInImage24Bit(img, w, h, x0, y0, x1, y1, lw, RGBA(r, g, b));
 }

@@ -4,11 +4,11 @@ The same operation sequence (volume, spacing, direction, label masks,
 transfer-function control points, windows, caps, camera, VR size, MPR type
 and thickness, crosshair moves, CPR path and rotation) drives MonkeyGL's own
 HelloMonkey (its host code and kernels, built unmodified into
-oracle/_ref/libmkref_full.so) and this library's pyMonkeyGL.  VR images must
-match everywhere except the bottom-right 64x64 box, where MonkeyGL draws its
-orientation-box overlay on the CPU after the kernel (core/VRImageLayer.cpp:
-104-155), which this library does not draw; planes and CPR images must match
-exactly."""
+oracle/_ref/libmkref_full.so) and this library's pyMonkeyGL.  VR images,
+with MonkeyGL's overlays (the orientation box in the bottom-right 64x64
+pixels, drawn from ./resources/human.stl, and the CPR line), planes and CPR
+images must match exactly.  Both HelloMonkey objects are constructed in the
+directory holding resources/, where MonkeyGL expects its mesh."""
 import ctypes as C
 import sys
 from pathlib import Path
@@ -71,12 +71,21 @@ def run_both(p, ops, masks=None):
     """Apply `ops` to MonkeyGL's HelloMonkey and to pyMonkeyGL; return both."""
     ref = RefHelloMonkey()
     L, h = ref.L, ref.h
-    mine = pm.HelloMonkey()
+    import os
+    cwd = os.getcwd()
+    os.chdir(FULL.parent)       # ./resources/human.stl, as for MonkeyGL's object
+    try:
+        mine = pm.HelloMonkey()
+    finally:
+        os.chdir(cwd)
     X, Y, Z = p.dims
     L.mkrh_set_volume(h, ptr(p.volume), X, Y, Z)
     mine.SetVolumeArray(p.volume.swapaxes(2, 0))
     d = np.array([1, 0, 0, 0, 1, 0, 0, 0, -1], np.float64)
     L.mkrh_set_direction(h, ptr(d))
+    # MonkeyGL's process-wide state keeps the last CPR path, whose line
+    # layer it draws into every VR image; each test starts without one
+    L.mkrh_set_cpr_line_voxel(h, ptr(np.zeros((1, 3), np.float64)), 0)
     mine.SetDirection(pm.Direction3d(1, 0, 0), pm.Direction3d(0, 1, 0), pm.Direction3d(0, 0, -1))
     L.mkrh_set_spacing(h, *p.spacing)
     mine.SetSpacing(*p.spacing)
@@ -161,12 +170,11 @@ def ref_plane(ref, plane):
 
 def assert_vr_equal(a, b, what):
     assert a.shape == b.shape, (a.shape, b.shape)
-    h, w = a.shape[:2]
-    keep = np.ones((h, w), bool)
-    if w > 64 and h > 64:
-        keep[h - 64:, w - 64:] = False
     d = np.abs(a.astype(int) - b.astype(int)).max(-1)
-    assert (d[keep] == 0).all(), f"{what}: {int((d[keep] > 0).sum())} pixels differ, max {int(d[keep].max())}"
+    h, w = a.shape[:2]
+    box = d[h - 64:, w - 64:] if w > 64 and h > 64 else d[:0]
+    assert (d == 0).all(), (f"{what}: {int((d > 0).sum())} pixels differ ({int((box > 0).sum())} in the "
+                            f"orientation box), max {int(d.max())}")
 
 
 @pytest.fixture(scope="module")
@@ -187,6 +195,19 @@ def test_default_windows_render_background(phantom):
     img = mine.GetVRImage()
     assert_vr_equal(img, ref_vr(ref), "default windows")
     assert (img[:200, :200] == [51, 76, 102]).all()
+
+
+# Before any label mask exists in MonkeyGL's process-wide state (see above).
+def test_cpr_line_layer_in_vr(phantom):
+    # the VR image carries the CPR path as a white 1-pixel polyline over the
+    # orientation box and the ray-cast image
+    line = [[20.0 + 3.0 * i, 30.0 + 8.0 * np.sin(i / 4.0), 10.0 + 2.5 * i] for i in range(30)]
+    ops = [("cpr_line", line), ("rotate_cpr", 30, 7), ("tf", TF4, {}, -1), ("wwwl", 1700, 650, -1),
+           ("rotate", 40, 0)]
+    ref, mine = run_both(phantom, ops)
+    img = mine.GetVRImage()
+    assert_vr_equal(img, ref_vr(ref), "VR with the CPR line layer")
+    assert ((img == 255).all(-1)).sum() >= 100, "no CPR line drawn"
 
 
 @pytest.mark.parametrize("rtype", [0, 1, 2])
