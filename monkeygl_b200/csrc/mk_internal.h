@@ -89,6 +89,15 @@ struct VolumeState {
     TileOrder orders[16] = {};
     int n_orders = 0;
 
+    // ray parameter (accu[k] - 0.866) * scale of every schedule entry, per
+    // camera scale: samples on the table read it instead of evaluating it
+    struct FyTable {
+        float scale;
+        float *d_fy;
+    };
+    FyTable fy_tables[8] = {};
+    int n_fy_tables = 0;
+
     size_t device_bytes = 0;
 };
 

@@ -15,6 +15,8 @@
 #pragma once
 
 #include <math.h>
+#include <stdint.h>
+#include <string.h>
 
 #if defined(__CUDACC__)
 #define MK_HD __host__ __device__ __forceinline__
@@ -77,15 +79,114 @@ MK_HD void sub_dconst(float x, dconst c, float &h, float &l) {
     two_sum(u, MK_ADD_RN(ue, t2), h, l);
 }
 
+// float <-> bits and leading zeros, on both sides of the compiler.
+MK_HD uint32_t float_bits(float f) {
+#if defined(__CUDA_ARCH__)
+    return __float_as_uint(f);
+#else
+    uint32_t u;
+    memcpy(&u, &f, sizeof(u));
+    return u;
+#endif
+}
+
+MK_HD float bits_float(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+    return __uint_as_float(u);
+#else
+    float f;
+    memcpy(&f, &u, sizeof(f));
+    return f;
+#endif
+}
+
+MK_HD int clz64(uint64_t x) {
+#if defined(__CUDA_ARCH__)
+    return __clzll((long long)x);
+#else
+    return __builtin_clzll(x);
+#endif
+}
+
+// Round the unsigned integer q (q > 0) to `bits` significant bits, ties to
+// even; the result is m * 2^e with m < 2^bits.
+MK_HD void round_bits(unsigned __int128 q, int bits, unsigned __int128 &m, int &e) {
+    const uint64_t hi = (uint64_t)(q >> 64), lo = (uint64_t)q;
+    const int len = hi ? 128 - clz64(hi) : 64 - clz64(lo);
+    if (len <= bits) {
+        m = q;
+        e = 0;
+        return;
+    }
+    const int sh = len - bits;
+    unsigned __int128 r = q >> sh;
+    const unsigned __int128 rem = q & ((((unsigned __int128)1) << sh) - 1);
+    const unsigned __int128 half = ((unsigned __int128)1) << (sh - 1);
+    if (rem > half || (rem == half && (r & 1))) r += 1;
+    e = sh;
+    if (r >> bits) {   // carried into a new bit
+        r >>= 1;
+        e += 1;
+    }
+    m = r;
+}
+
+// The same product by integers: for a == 0 or a >= 2^-30 (every
+// accuLength of the schedule) (double)a - 0.866 is exactly N * 2^-53 with
+// |N| < 2^53, so with scale = S * 2^k (24-bit S) the product is the integer
+// N * S * 2^(k - 53), at most 77 bits; rounding it to 53 and then to 24
+// significant bits, ties to even each time, reproduces both of MonkeyGL's
+// roundings exactly.  Returns false for other a (never produced).
+MK_HD bool ray_fy_exact(float a, float scale, float &out) {
+    const uint32_t ab = float_bits(a), sb = float_bits(scale);
+    const int ea = (int)((ab >> 23) & 255), es = (int)((sb >> 23) & 255);
+    if (!((a == 0.0f || (ea >= 127 - 30 && ea < 255)) && es > 0 && es < 255)) return false;
+    // 0.866 = C * 2^-53 exactly (its double significand)
+    const int64_t C = (int64_t)(0.866 * 9007199254740992.0);
+    int64_t n = -C;
+    if (a != 0.0f) {
+        const int64_t ma = (int64_t)((ab & 0x7fffff) | 0x800000);   // a = ma * 2^(ea - 150)
+        const int64_t va = ma << (ea - 150 + 53);                    // a * 2^53, exact
+        n = ((ab >> 31) ? -va : va) - C;
+    }
+    const bool neg = (n < 0) != ((sb >> 31) != 0);
+    const uint64_t un = (uint64_t)(n < 0 ? -n : n);
+    const uint64_t ms = (uint64_t)((sb & 0x7fffff) | 0x800000);   // scale = ms * 2^(es - 150)
+    const unsigned __int128 q = (unsigned __int128)un * ms;       // |product| = q * 2^(es - 150 - 53)
+    unsigned __int128 m53, m24;
+    int e53, e24;
+    round_bits(q, 53, m53, e53);
+    round_bits(m53, 24, m24, e24);
+    const float r = ldexpf((float)(uint32_t)m24, e53 + e24 + es - 150 - 53);
+    out = neg ? -r : r;
+    return true;
+}
+
 // (float)(((double)a - 0.866) * (double)scale): the ray parameter of
-// core/kernel.cu:197 (and :313, :415), whose 0.866 literal is a double.
+// core/kernel.cu:197 (and :313, :415), whose 0.866 literal makes the
+// expression double: the product is rounded to 53 bits, then to 24.  The
+// float evaluation below carries the product to within 2^-47 of its value
+// and rounds once.  Where the carried product lies more than 2^-20 half-ulps
+// (2^-44 relative, eight times that error) from a float rounding midpoint,
+// the exact product is on the same side of it and outside the 2^-53 window
+// where rounding to double first could land on the midpoint, so both
+// evaluations give this float; the residual of the final rounding measures
+// that distance.  The rest (about one product in 2^20) take the exact
+// integer route.
 MK_HD float ray_fy(float a, float scale) {
     float h, l;
     sub_dconst(a, MK_DCONST(0.866), h, l);
     float p, pe;
     two_prod(h, scale, p, pe);
     pe = MK_FMA(l, scale, pe);
-    return MK_ADD_RN(p, pe);
+    const float r = MK_ADD_RN(p, pe);
+    // residual of that rounding (|pe| <= ulp(p), so this is exact)
+    const float e = MK_ADD_RN(MK_ADD_RN(p, -r), pe);
+    const float half_ulp = MK_MUL_RN(mk::bits_float(float_bits(r) & 0x7f800000u), 5.9604645e-08f);   // 2^-24
+    const float d = fabsf(MK_ADD_RN(fabsf(e), -half_ulp));
+    if (d > MK_MUL_RN(half_ulp, 9.5367432e-07f)) return r;   // 2^-20 half-ulps from a midpoint
+    float x;
+    return ray_fy_exact(a, scale, x) ? x : r;
 }
 
 // (float)((double)x + c) for a double constant c, e.g. the "+0.05" of

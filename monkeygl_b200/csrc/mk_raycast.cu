@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <algorithm>
 #include <utility>
@@ -142,6 +143,44 @@ static int tile_order(VolumeState &v, const RayParams &P, cudaStream_t s, const 
     return MK_OK;
 }
 
+// fy = (accu[k] - 0.866) * scale for every schedule entry, by the same
+// device function the kernels evaluate per sample (core/kernel.cu:197).
+__global__ void k_fy_table(const float *__restrict__ accu, int n, float scale, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = ray_fy(accu[i], scale);
+}
+
+// The fy table of volume v at `scale`, cached on the volume (8 scales).  A
+// new table is built on `s` and waited for once, so launches on other
+// streams can share it.
+static int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out) {
+    for (int i = 0; i < v.n_fy_tables; ++i) {
+        if (memcmp(&v.fy_tables[i].scale, &scale, sizeof(float)) == 0) {
+            *out = v.fy_tables[i].d_fy;
+            return MK_OK;
+        }
+    }
+    if (v.n_fy_tables == 8) {   // drop the oldest
+        MK_CUDA_TRY(cudaStreamSynchronize(s));
+        cudaFree(v.fy_tables[0].d_fy);
+        for (int i = 1; i < 8; ++i) v.fy_tables[i - 1] = v.fy_tables[i];
+        v.n_fy_tables = 7;
+    }
+    float *d = nullptr;
+    MK_CUDA_TRY(cudaMalloc(&d, (size_t)v.accu_len * sizeof(float)));
+    k_fy_table<<<(v.accu_len + 255) / 256, 256, 0, s>>>(v.d_accu, v.accu_len, scale, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        set_last_error(std::string("fy table: ") + cudaGetErrorString(e));
+        return MK_ERR_CUDA;
+    }
+    v.fy_tables[v.n_fy_tables++] = {scale, d};
+    *out = d;
+    return MK_OK;
+}
+
 // Labels that need a per-ray opacity accumulator: present in the mask and
 // with a cap strictly between 0 and 1.
 int tracking_mode_for(const uint64_t present[2], const float (*params)[3]) {
@@ -194,6 +233,7 @@ int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P) {
     P.step1 = 1.0f / (float)v.dims[2];
     P.limit = float_bound_above(1.732);
     P.accu = v.d_accu;
+    P.fy_tab = nullptr;
     P.accu_len = v.accu_len;
     P.rgba = (p->pixel_format == MK_PIXEL_RGBA8) ? 1 : 0;
     P.skip = (p->flags & MK_VR_NO_SKIP) ? 0 : 1;
@@ -233,6 +273,8 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     if (rc != MK_OK) return rc;
     const int *order = nullptr;
     rc = tile_order(v, P, s, &order);
+    if (rc != MK_OK) return rc;
+    rc = fy_table(v, P.scale, s, &P.fy_tab);
     if (rc != MK_OK) return rc;
     launch_raycast<false>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
                           label_table(&v), brick_view(&v), order, s);

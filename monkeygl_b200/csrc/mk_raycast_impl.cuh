@@ -32,6 +32,7 @@ struct RayParams {
     float step1;                 // 1 / dim_z
     float limit;                 // smallest float > 1.732
     const float *accu;           // accuLength schedule table
+    const float *fy_tab;         // ray parameter of each table entry at this scale (null: compute)
     int accu_len;
     int rgba;                    // 1 = 4 bytes per pixel
     int skip;
@@ -60,18 +61,31 @@ __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, fl
     return __fmaf_rn(az, bz, __fmaf_rn(ay, by, __fmul_rn(ax, bx)));
 }
 
-// One sample position of the reference schedule (core/kernel.cu:197-206).
-__device__ __forceinline__ float3 ray_pos(const RayParams &P, float u, float v, float a) {
-    const float fy = ray_fy(a, P.scale);
+// One sample position of the reference schedule (core/kernel.cu:197-206)
+// from the ray parameter fy = (accuLength - 0.866) * scale.
+__device__ __forceinline__ float3 ray_pos_fy(const RayParams &P, float u, float v, float fy) {
     float3 p;
     p.x = dot3(u, fy, v, P.M[0], P.M[1], P.M[2]);
     p.y = dot3(u, fy, v, P.M[3], P.M[4], P.M[5]);
     p.z = dot3(u, fy, v, P.M[6], P.M[7], P.M[8]);
-    p.x = p.x * P.mls[0] + 0.5f;
-    p.y = p.y * P.mls[1] + 0.5f;
-    p.z = p.z * P.mls[2] + 0.5f;
+    // pos * maxLenSpacing + 0.5: fused, as nvcc compiles MonkeyGL's
+    // expression (a separate multiply and add misplaces samples); written
+    // out so that no inlining context can change it
+    p.x = __fmaf_rn(p.x, P.mls[0], 0.5f);
+    p.y = __fmaf_rn(p.y, P.mls[1], 0.5f);
+    p.z = __fmaf_rn(p.z, P.mls[2], 0.5f);
     if (P.invertZ) p.z = 1.0f - p.z;
     return p;
+}
+
+__device__ __forceinline__ float3 ray_pos(const RayParams &P, float u, float v, float a) {
+    return ray_pos_fy(P, u, v, ray_fy(a, P.scale));
+}
+
+// The position of a sample that lies on the schedule table (a == accu[k]):
+// its ray parameter comes from the frame's table when there is one.
+__device__ __forceinline__ float3 ray_pos_at(const RayParams &P, float u, float v, int k, float a) {
+    return P.fy_tab ? ray_pos_fy(P, u, v, P.fy_tab[k]) : ray_pos(P, u, v, a);
 }
 
 // Interval [a0, a1] of accuLength where the ray may touch the VOI, from the
@@ -436,13 +450,14 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             int flags = 0, label = 0, nskip = 0;
             if (!Q.done) {
                 float aj = Q.a;
-                if (Q.lat >= 0) aj = P.accu[min(Q.lat + j, P.accu_len - 1)];
+                const int kj = Q.lat >= 0 ? min(Q.lat + j, P.accu_len - 1) : -1;
+                if (kj >= 0) aj = P.accu[kj];
                 else
                     for (int k = 0; k < j; ++k) aj += Q.step;
                 if (!(aj < P.limit) || aj > Q.a_stop) {
                     flags = kCoopEnd;
                 } else {
-                    const float3 pos = ray_pos(P, Q.u, Q.v, aj);
+                    const float3 pos = kj >= 0 ? ray_pos_at(P, Q.u, Q.v, kj, aj) : ray_pos(P, Q.u, Q.v, aj);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
@@ -633,7 +648,7 @@ __device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject
                 R.done = true;
                 break;
             }
-            const float3 pos = ray_pos(P, R.u, R.v, R.a);
+            const float3 pos = R.lat >= 0 ? ray_pos_at(P, R.u, R.v, R.lat, R.a) : ray_pos(P, R.u, R.v, R.a);
             const int ix = pos.x * P.fdim[0];
             const int iy = pos.y * P.fdim[1];
             const int iz = pos.z * P.fdim[2];
@@ -798,25 +813,27 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                 }
                 if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;
             } else if (MODE == kModeMIP) {
-                const float fStep = P.step1;
+                // fixed step 1/dim_z from a table entry: every sample is
+                // table entry k, a == accu[k]
+                int k = k0;
                 while (a < P.limit) {
                     if (a > a_stop) break;
-                    const float3 pos = ray_pos(P, u, v, a);
+                    const float3 pos = ray_pos_at(P, u, v, k, a);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
                     if (outside_voi(P, ix, iy, iz)) {
-                        a += fStep;
+                        k = min(k + 1, P.accu_len - 1);
+                        a = P.accu[k];
                         continue;
                     }
                     if (!COUNT && P.skip) {
                         const int b = brick_index(P, BV, ix, iy, iz);
                         if (BV.mip_tmax[b] <= A) {
-                            a += fStep;
                             const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1],
                                                           pos.z * P.fdim[2]);
-                            int n = steps_in_brick(pv, dv, ix, iy, iz);
-                            for (; n > 0; --n) a += fStep;
+                            k = min(k + 1 + steps_in_brick(pv, dv, ix, iy, iz), P.accu_len - 1);
+                            a = P.accu[k];
                             continue;
                         }
                     }
@@ -831,14 +848,14 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                         temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
                         if (A < temp) A = temp;
                     }
-                    a += fStep;
+                    k = min(k + 1, P.accu_len - 1);
+                    a = P.accu[k];
                     // the output saturates at 1.0 (core/kernel.cu:351-358)
                     if (!COUNT && P.skip && A >= 1.0f) break;
                 }
                 if (A <= 0.0f) sum = P.bg;
                 else sum = make_float4(A, A, A, A);
             } else {   // kModeSurface
-                const float fStep = P.step1;
                 float3 L;
                 {
                     float lx_ = dot3(0.0f, 1.0f, 0.0f, P.M[0], P.M[1], P.M[2]);
@@ -847,14 +864,17 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                     const float inv = rsqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_);
                     L = make_float3(lx_ * inv, ly_ * inv, lz_ * inv);
                 }
+                // fixed step from a table entry, as for MIP
+                int k = k0;
                 while (a < P.limit) {
                     if (a > a_stop) break;
-                    const float3 pos = ray_pos(P, u, v, a);
+                    const float3 pos = ray_pos_at(P, u, v, k, a);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
                     if (outside_voi(P, ix, iy, iz)) {
-                        a += fStep;
+                        k = min(k + 1, P.accu_len - 1);
+                        a = P.accu[k];
                         continue;
                     }
                     if (!COUNT && P.skip) {
@@ -862,11 +882,10 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                         const short2 mm = BV.minmax[b];
                         // 32768 * (v / 32767) <= 400 for every tap
                         if ((float)mm.y * (32768.0f / 32767.0f) + 0.01f <= 400.0f) {
-                            a += fStep;
                             const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1],
                                                           pos.z * P.fdim[2]);
-                            int n = steps_in_brick(pv, dv, ix, iy, iz);
-                            for (; n > 0; --n) a += fStep;
+                            k = min(k + 1 + steps_in_brick(pv, dv, ix, iy, iz), P.accu_len - 1);
+                            a = P.accu[k];
                             continue;
                         }
                     }
@@ -876,7 +895,8 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                     }
                     const float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
                     if (temp <= 400) {
-                        a += fStep;
+                        k = min(k + 1, P.accu_len - 1);
+                        a = P.accu[k];
                         continue;
                     }
                     if (COUNT) mark_gradient(P, pos);
@@ -891,7 +911,8 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                     N.z = N.z * inv;
                     A = N.x * L.x + N.y * L.y + N.z * L.z;
                     if (A > 0) break;
-                    a += fStep;
+                    k = min(k + 1, P.accu_len - 1);
+                    a = P.accu[k];
                 }
                 if (A <= 0.0f) {
                     sum = P.bg;

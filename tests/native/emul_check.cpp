@@ -18,6 +18,19 @@ int64_t check_ray_fy(const float *a, const float *scale, int64_t n, float *emul,
     return bad;
 }
 
+// the exact integer route alone (ray_fy takes it near rounding midpoints)
+int64_t check_ray_fy_exact(const float *a, const float *scale, int64_t n, float *emul, float *ref) {
+    int64_t bad = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        float x = 0.0f;
+        if (!mk::ray_fy_exact(a[i], scale[i], x)) x = -1e30f;
+        emul[i] = x;
+        ref[i] = (float)(((double)a[i] - 0.866) * (double)scale[i]);
+        bad += emul[i] != ref[i];
+    }
+    return bad;
+}
+
 // (float)((double)x + 0.05)
 int64_t check_add005(const float *x, int64_t n, float *emul, float *ref) {
     int64_t bad = 0;

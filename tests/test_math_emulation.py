@@ -27,7 +27,7 @@ def lib():
         subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",
                         f"-I{hdr.parent}", str(SRC), "-o", str(so)], check=True)
     L = C.CDLL(str(so))
-    for f in ("check_ray_fy", "check_add005", "check_cpr", "check_mean"):
+    for f in ("check_ray_fy", "check_ray_fy_exact", "check_add005", "check_cpr", "check_mean"):
         getattr(L, f).restype = C.c_int64
     return L
 
@@ -49,9 +49,30 @@ def test_ray_parameter_matches_double(lib):
     e = np.empty_like(a)
     r = np.empty_like(a)
     bad = lib.check_ray_fy(p(a), p(scale), a.size, p(e), p(r))
-    # double rounding in MonkeyGL's own evaluation can differ from the correctly
-    # rounded value only at exact float midpoints: allow one in a million
-    assert bad <= a.size // 1_000_000 + 1, bad
+    assert bad == 0, bad
+
+
+def test_ray_parameter_double_rounding_cases(lib):
+    # inputs whose product lies next to a float rounding midpoint, where
+    # MonkeyGL's two roundings (to double, then to float) differ from one
+    # correct rounding; found by an exhaustive search over all floats in
+    # [2^-12, 1.732] at these scales
+    cases = [(0x3e79999b, 1.3), (0x3db851e5, 0.8), (0x3db851ef, 0.8), (0x3d449242, 0.4321),
+             (0x3e179e87, 0.4321), (0x39b5c183, 1.1), (0x3a3adf4d, 1.1)]
+    a = np.array([c[0] for c in cases], np.uint32).view(np.float32)
+    scale = np.array([c[1] for c in cases], np.float32)
+    e = np.empty_like(a)
+    r = np.empty_like(a)
+    assert lib.check_ray_fy(p(a), p(scale), a.size, p(e), p(r)) == 0, list(zip(e, r))
+
+
+def test_ray_parameter_integer_route_matches_double(lib):
+    rng = np.random.default_rng(5)
+    a = np.concatenate([[0.0], rng.uniform(2.0 ** -30, 1.75, 1_000_000)]).astype(np.float32)
+    scale = np.exp(rng.uniform(-3, 3, a.size)).astype(np.float32)
+    e = np.empty_like(a)
+    r = np.empty_like(a)
+    assert lib.check_ray_fy_exact(p(a), p(scale), a.size, p(e), p(r)) == 0
 
 
 def test_surface_offset_matches_double(lib):
