@@ -40,12 +40,13 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "VR fps & Gsamples/s vs ref CUDA on 1xB200; served p50/p99 ms; bwd/fwd time"
+MODES = {"vr": 0, "mip": 1, "surface": 2}
 WORKLOADS = {
-    "body": ("body VR: int16 512x512x1559 (0.7422x0.7422x1.0 mm), 4 labelled objects + background "
+    "body": ("body {mode}: int16 512x512x1559 (0.7422x0.7422x1.0 mm), 4 labelled objects + background "
              "(cap {bg}), 256-entry LUT per label, {size}x{size} RGB8, 36 views about z"),
-    "cardiac": ("cardiac VR: int16 512x512x361 (0.351x0.351x0.3 mm), one 256-entry LUT, "
+    "cardiac": ("cardiac {mode}: int16 512x512x361 (0.351x0.351x0.3 mm), one 256-entry LUT, "
                 "{size}x{size} RGB8, 36 views about z"),
-    "small": ("small VR: int16 128x128x96 (0.35x0.35x0.3 mm), one 256-entry LUT, {size}x{size} RGB8, "
+    "small": ("small {mode}: int16 128x128x96 (0.35x0.35x0.3 mm), one 256-entry LUT, {size}x{size} RGB8, "
               "3 views about z"),
 }
 
@@ -59,6 +60,8 @@ def parse_args():
     ap.add_argument("--bg", type=float, default=0.4)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="body")
     ap.add_argument("--size", type=int, default=1024)
+    ap.add_argument("--mode", choices=["vr", "mip", "surface"], default="vr",
+                    help="render type of the timed frames (the contract line is VR)")
     ap.add_argument("--suite", action="store_true")
     ap.add_argument("--suite-only", default="", help="comma list of suite groups: vr,mpr,cpr,dvr (default all)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (monkeygl_b200.serve_bench)")
@@ -225,7 +228,7 @@ def frame_params(w, angle, size, render_type=0):
     return capi.vr_params(size, size, render_type, view_camera(angle), w.dims, w.spacing, invert_z=False)
 
 
-def cpu_baseline(w, angle, size):
+def cpu_baseline(w, angle, size, rtype=0):
     """Time the C restatement (oracle, texture-emulating FP32): whole frames
     of consecutive views with OpenMP over rows on every host thread for about
     10 s, and one thread on every 16th row of a frame (scaled to a frame)."""
@@ -240,15 +243,15 @@ def cpu_baseline(w, angle, size):
     start = angles.index(angle) if angle in angles else 0
     while True:
         a = angles[(start + frames) % len(angles)]
-        flat = capi.vr_params_flat(frame_params(w, a, size), w.label_params)
-        cv.render_vr(size, size, 0, flat, threads=cores)
+        flat = capi.vr_params_flat(frame_params(w, a, size, rtype), w.label_params)
+        cv.render_vr(size, size, rtype, flat, threads=cores)
         frames += 1
         dt = time.perf_counter() - t0
         if dt >= 10.0 or frames >= 2 * len(angles):
             break
-    flat = capi.vr_params_flat(frame_params(w, angles[start], size), w.label_params)
+    flat = capi.vr_params_flat(frame_params(w, angles[start], size, rtype), w.label_params)
     t1 = time.perf_counter()
-    cv.render_vr_rows(size, size, 0, flat, 0, 16, size // 16, threads=1)
+    cv.render_vr_rows(size, size, rtype, flat, 0, 16, size // 16, threads=1)
     one = (time.perf_counter() - t1) * 16
     return {"value": round(frames / dt, 4), "unit": "fps", "cores": cores, "kind": "port",
             "single_thread_fps": round(1.0 / one, 5),
@@ -268,7 +271,8 @@ def run_mine(args, rank, local, world):
     vol = setup_volume(w, local)
     angles = w.angles
     views = rank_views(angles, rank)
-    params = [frame_params(w, a, size) for a in views]
+    rtype = MODES[args.mode]
+    params = [frame_params(w, a, size, rtype) for a in views]
     stream = torch.cuda.Stream()
     out = torch.empty(size * size * 3, dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -332,7 +336,7 @@ def run_mine(args, rank, local, world):
         "metric": METRIC, "value": round(value, 3), "unit": "fps", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": round(total_max * 1e3 / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload].format(bg=args.bg, size=size), "views": len(angles), "image": f"{size}x{size}",
+        "config": {"workload": WORKLOADS[args.workload].format(bg=args.bg, size=size, mode=args.mode.upper()), "views": len(angles), "image": f"{size}x{size}",
                    "bg_alpha": args.bg, "l2": "flushed between steps (256 MiB write, outside the events)",
                    "parallelism": f"replicas{world}" if world > 1 else "single GPU"},
         "gsamples_per_s": round(gsps * world, 3),
@@ -345,12 +349,12 @@ def run_mine(args, rank, local, world):
                      "frac": round(achieved / peak, 4), "traffic": traffic_from_profile(),
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
                      "algorithmic_bytes_per_launch": int(b_alg),
-                     "kernel": "mk::k_raycast<VR, shared caps> (one launch per frame)"},
+                     "kernel": f"mk::k_raycast<{args.mode.upper()}> (one launch per frame)"},
         "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons", "samples")},
         "gpu_launches": K,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, views[0], size)
+        line["cpu_baseline"] = cpu_baseline(w, views[0], size, rtype)
     vol.close()
     return line
 
@@ -377,27 +381,27 @@ def run_reference(args, rank, world):
         ref.set_lut(l, lut)
     flats = []
     for a in w.angles:
-        p = frame_params(w, a, size)
+        p = frame_params(w, a, size, MODES[args.mode])
         flats.append(np.ascontiguousarray(capi.vr_params_flat(p, w.label_params)))
     K, W = args.steps, max(3, args.warmup)
     out = np.zeros((size, size, 3), np.uint8)
     for i in range(W):
-        ref.render_into(out, size, size, 0, flats[i % len(flats)])
+        ref.render_into(out, size, size, MODES[args.mode], flats[i % len(flats)])
     clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
     clocks.start()
     t0 = time.perf_counter()
     for i in range(K):
-        ref.render_into(out, size, size, 0, flats[i % len(flats)])
+        ref.render_into(out, size, size, MODES[args.mode], flats[i % len(flats)])
     dt = time.perf_counter() - t0
     clk = clocks.stop()
-    kms = float(np.mean([ref.kernel_ms(size, size, 0, flats[i], 3)
+    kms = float(np.mean([ref.kernel_ms(size, size, MODES[args.mode], flats[i], 3)
                          for i in sorted({(k * len(flats)) // 4 for k in range(4)})]))
     value = K / dt
     return {
         "metric": METRIC, "impl": "reference", "value": round(value, 3), "unit": "fps", "n_gpus": 1,
         "steps": K, "warmup": W, "ms_per_step": round(dt * 1e3 / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.workload].format(bg=args.bg, size=size), "views": len(w.angles), "image": f"{size}x{size}",
+        "config": {"workload": WORKLOADS[args.workload].format(bg=args.bg, size=size, mode=args.mode.upper()), "views": len(w.angles), "image": f"{size}x{size}",
                    "bg_alpha": args.bg, "l2": "inputs larger than L2 (817 MB volume)",
                    "parallelism": "single GPU"},
         "kernel_ms_per_frame": round(kms, 4),

@@ -37,81 +37,79 @@ struct DeviceGuard {
     }
 };
 
-// One block per brick: min/max of the int16 voxels in the brick grown by one
+// One warp per brick: min/max of the int16 voxels in the brick grown by one
 // voxel on every side (clamped to the volume), i.e. every voxel a trilinear
-// tap of an owned sample can touch.
+// tap of an owned sample can touch.  The grown brick is at most 10x10x10;
+// lanes 0-29 cover three of its 10-voxel rows at a time (lane = 10 * row +
+// column) and the warp walks its rows and slices, so the loads of a warp
+// are three short contiguous segments and no lane divides.  Bricks are
+// numbered x fastest, so neighbouring warps share their halo rows in L2.
 __global__ void __launch_bounds__(256) k_brick_minmax(const short *__restrict__ vox, int dx, int dy,
-                                                      int dz, int nbx, int nby, short2 *out) {
-    const int b = blockIdx.x;
+                                                      int dz, int nbx, int nby, int nbricks, short2 *out) {
+    const int b = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (b >= nbricks) return;
+    const int lane = threadIdx.x & 31;
     const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
     const int x0 = max(bx * kBrick - 1, 0), x1 = min(bx * kBrick + kBrick, dx - 1);
     const int y0 = max(by * kBrick - 1, 0), y1 = min(by * kBrick + kBrick, dy - 1);
     const int z0 = max(bz * kBrick - 1, 0), z1 = min(bz * kBrick + kBrick, dz - 1);
-    const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
-    const int total = nx * ny * nz;
+    const int col = lane % 10, row = lane / 10;   // row 3 (lanes 30, 31) idle
+    const int x = x0 + col;
     int lo = 32767, hi = -32768;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-        int x = x0 + i % nx;
-        int y = y0 + (i / nx) % ny;
-        int z = z0 + i / (nx * ny);
-        int v = vox[((size_t)z * dy + y) * dx + x];
-        lo = min(lo, v);
-        hi = max(hi, v);
+    if (row < 3 && x <= x1 && y0 + row <= y1) {
+        const size_t plane = (size_t)dy * dx, step = 3 * (size_t)dx;
+        const int nrows = (y1 - y0 - row) / 3 + 1;   // 3 or 4
+        const short *p = vox + (size_t)z0 * plane + (size_t)(y0 + row) * dx + x;
+        for (int z = z0; z <= z1; ++z, p += plane) {
+            const short *q = p;
+#pragma unroll 4
+            for (int r = 0; r < nrows; ++r, q += step) {
+                const int v = __ldg(q);
+                lo = min(lo, v);
+                hi = max(hi, v);
+            }
+        }
     }
     lo = __reduce_min_sync(0xffffffffu, lo);
     hi = __reduce_max_sync(0xffffffffu, hi);
-    __shared__ int s_lo[8], s_hi[8];
-    const int w = threadIdx.x >> 5;
-    if ((threadIdx.x & 31) == 0) {
-        s_lo[w] = lo;
-        s_hi[w] = hi;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
-            lo = min(lo, s_lo[i]);
-            hi = max(hi, s_hi[i]);
-        }
-        out[b] = make_short2((short)lo, (short)hi);
-    }
+    if (lane == 0) out[b] = make_short2((short)lo, (short)hi);
 }
 
-// One block per brick: the set of labels among the brick's owned voxels, as
-// a 65-bit mask in three words.
+// One warp per brick: the set of labels among the brick's owned voxels
+// (8x8x8 at most), as a 65-bit mask in three words.  Lane = 8 * row +
+// column covers four 8-byte rows at a time.
 __global__ void __launch_bounds__(256) k_brick_labels(const unsigned char *__restrict__ lab, int dx,
-                                                      int dy, int dz, int nbx, int nby,
+                                                      int dy, int dz, int nbx, int nby, int nbricks,
                                                       uint32_t *out) {
-    const int b = blockIdx.x;
+    const int b = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (b >= nbricks) return;
+    const int lane = threadIdx.x & 31;
     const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
     const int x0 = bx * kBrick, x1 = min(x0 + kBrick, dx) - 1;
     const int y0 = by * kBrick, y1 = min(y0 + kBrick, dy) - 1;
     const int z0 = bz * kBrick, z1 = min(z0 + kBrick, dz) - 1;
-    const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
-    const int total = nx * ny * nz;
+    const int x = x0 + (lane & 7), row = lane >> 3;
     uint32_t m0 = 0, m1 = 0, m2 = 0;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-        int x = x0 + i % nx;
-        int y = y0 + (i / nx) % ny;
-        int z = z0 + i / (nx * ny);
-        int l = lab[((size_t)z * dy + y) * dx + x];
-        if (l > 64) l = 64;   // labels above MAXOBJECTCOUNT never occur via the API
-        if (l < 32) m0 |= 1u << l;
-        else if (l < 64) m1 |= 1u << (l - 32);
-        else m2 |= 1u;
+    if (x <= x1 && y0 + row <= y1) {
+        const size_t plane = (size_t)dy * dx, step = 4 * (size_t)dx;
+        const int nrows = (y1 - y0 - row) / 4 + 1;   // 1 or 2
+        const unsigned char *p = lab + (size_t)z0 * plane + (size_t)(y0 + row) * dx + x;
+        for (int z = z0; z <= z1; ++z, p += plane) {
+            const unsigned char *q = p;
+#pragma unroll 2
+            for (int r = 0; r < nrows; ++r, q += step) {
+                int l = __ldg(q);
+                if (l > 64) l = 64;   // labels above MAXOBJECTCOUNT never occur via the API
+                if (l < 32) m0 |= 1u << l;
+                else if (l < 64) m1 |= 1u << (l - 32);
+                else m2 |= 1u;
+            }
+        }
     }
     m0 = __reduce_or_sync(0xffffffffu, m0);
     m1 = __reduce_or_sync(0xffffffffu, m1);
     m2 = __reduce_or_sync(0xffffffffu, m2);
-    __shared__ uint32_t s[3];
-    if (threadIdx.x < 3) s[threadIdx.x] = 0;
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) {
-        atomicOr(&s[0], m0);
-        atomicOr(&s[1], m1);
-        atomicOr(&s[2], m2);
-    }
-    __syncthreads();
-    if (threadIdx.x < 3) out[3 * (size_t)b + threadIdx.x] = s[threadIdx.x];
+    if (lane < 3) out[3 * (size_t)b + lane] = lane == 0 ? m0 : (lane == 1 ? m1 : m2);
 }
 
 __global__ void k_fill_labels_zero(uint32_t *out, int nbricks) {
@@ -438,9 +436,8 @@ extern "C" int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x
         st.device_bytes += nbricks * (sizeof(short2) + 3 * sizeof(uint32_t) + sizeof(float)) +
                            nwords * sizeof(uint32_t) + sizeof(unsigned long long);
         cudaMemsetAsync(st.d_visible, 0, nwords * sizeof(uint32_t), st.stream);
-        k_brick_minmax<<<(unsigned)nbricks, 256, 0, st.stream>>>((const short *)d_lin, dim_x, dim_y,
-                                                                 dim_z, st.nb[0], st.nb[1],
-                                                                 st.d_minmax);
+        k_brick_minmax<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
+            (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], (int)nbricks, st.d_minmax);
         k_fill_labels_zero<<<(unsigned)((nbricks + 255) / 256), 256, 0, st.stream>>>(
             st.d_labels, (int)nbricks);
         e = cudaGetLastError();
@@ -506,6 +503,7 @@ extern "C" int mk_volume_destroy(mk_volume v) {
     cudaFree(st.d_out);
     cudaFree(st.d_counter);
     for (int i = 0; i < st.n_orders; ++i) cudaFree(st.orders[i].d_tiles);
+    for (int i = 0; i < st.n_fy_tables; ++i) cudaFree(st.fy_tables[i].d_fy);
     if (st.h_pinned) cudaFreeHost(st.h_pinned);
     if (st.stream) cudaStreamDestroy(st.stream);
     cudaGetLastError();
@@ -575,9 +573,8 @@ extern "C" int mk_volume_set_mask(mk_volume v, const uint8_t *labels) {
         }
     }
     if (rc == MK_OK) {
-        k_brick_labels<<<(unsigned)nbricks, 256, 0, st.stream>>>((const unsigned char *)d_lin, dx,
-                                                                 dy, dz, st.nb[0], st.nb[1],
-                                                                 st.d_labels);
+        k_brick_labels<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
+            (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], (int)nbricks, st.d_labels);
         e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaStreamSynchronize(st.stream);
         if (e != cudaSuccess) {
