@@ -63,7 +63,7 @@ def parse_args():
     ap.add_argument("--mode", choices=["vr", "mip", "surface"], default="vr",
                     help="render type of the timed frames (the contract line is VR)")
     ap.add_argument("--suite", action="store_true")
-    ap.add_argument("--suite-only", default="", help="comma list of suite groups: vr,mpr,cpr,dvr (default all)")
+    ap.add_argument("--suite-only", default="", help="comma list of suite groups: vr,mpr,cpr,dvr,api (default all)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (monkeygl_b200.serve_bench)")
     ap.add_argument("--serve-requests", type=int, default=10000)
     ap.add_argument("--serve-rate", type=float, default=200.0)
@@ -420,7 +420,9 @@ def main():
         import oracle
         from monkeygl_b200 import suite
         # MonkeyGL's own kernels built from its sources (oracle/_ref), for the reference columns
-        suite.main(args, oracle.RefGPU() if oracle.ref_gpu_available() else None)
+        suite.main(args, oracle.RefGPU() if oracle.ref_gpu_available() else None,
+                   oracle.RefHelloMonkey() if oracle.ref_full_available() else None,
+                   str(oracle.REF_FULL_LIB.parent) if oracle.ref_full_available() else None)
         return
     if args.serve:
         from monkeygl_b200 import serve_bench

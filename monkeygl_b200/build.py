@@ -27,7 +27,7 @@ NVCC_FLAGS = ARCH + [
     "-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
     "-Xcompiler", "-fPIC,-O3", f"-I{ROOT / 'include'}", f"-I{CSRC}",
 ]
-CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off",
+CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp",
              f"-I{ROOT / 'include'}", f"-I{CSRC}", "-I/usr/local/cuda/include"]
 
 
@@ -84,7 +84,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if force or jobs or not lib.exists() or lib.stat().st_mtime < _newest(objs):
         tmp = lib.with_suffix(".so.tmp")
         cmd = [NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", str(tmp)] + \
-              [str(o) for o in objs] + ["-lcudart_static", "-lrt", "-lpthread", "-ldl", "-lz"]
+              [str(o) for o in objs] + ["-lcudart_static", "-lrt", "-lpthread", "-ldl", "-lz", "-lgomp"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

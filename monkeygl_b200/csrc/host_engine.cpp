@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1190,8 +1192,35 @@ bool Engine::RenderVR(std::shared_ptr<unsigned char> &out, int &w, int &h) {
     w = p.width;
     h = p.height;
     out.reset(new unsigned char[(size_t)w * h * 3], std::default_delete<unsigned char[]>());
-    if (mk_render_vr(dev_, &p, out.get(), 0, nullptr) != MK_OK) return false;
-    if (mesh_) mk_merge_orientation_box(mesh_, rot_, out.get(), w, h);
+    // the orientation box is host work: it is drawn into a 65x65 scratch
+    // image (the box fills its bottom-right 64x64) on another thread while
+    // the GPU renders, then its drawn pixels (never black) are copied over
+    const bool box = mesh_ && w > 64 && h > 64;
+    std::vector<unsigned char> scratch;
+    std::thread worker;
+    if (box) {
+        scratch.assign(65 * 65 * 3, 0);
+        std::array<float, 9> rot;
+        std::memcpy(rot.data(), rot_, sizeof(rot_));
+        worker = std::thread([this, rot, &scratch] {
+            mk_merge_orientation_box(mesh_, rot.data(), scratch.data(), 65, 65);
+        });
+    }
+    const int rc = mk_render_vr(dev_, &p, out.get(), 0, nullptr);
+    if (worker.joinable()) worker.join();
+    if (rc != MK_OK) return false;
+    if (box) {
+        for (int j = 0; j < 64; ++j) {
+            const unsigned char *src = &scratch[((size_t)(j + 1) * 65 + 1) * 3];
+            unsigned char *dst = out.get() + ((size_t)(h - 64 + j) * w + (w - 64)) * 3;
+            for (int i = 0; i < 64; ++i)
+                if (src[3 * i] | src[3 * i + 1] | src[3 * i + 2]) {
+                    dst[3 * i] = src[3 * i];
+                    dst[3 * i + 1] = src[3 * i + 1];
+                    dst[3 * i + 2] = src[3 * i + 2];
+                }
+        }
+    }
     if (LayerEnabled(LayerTypeCPRLine) && cprLine_.size() >= 2) {
         const float clr[3] = {cprColor_.red, cprColor_.green, cprColor_.blue};
         float x0 = 0, y0 = 0, x1 = 0, y1 = 0;

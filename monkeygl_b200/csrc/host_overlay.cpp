@@ -28,7 +28,9 @@
 #include <stdio.h>
 #include <string.h>
 #include <sys/stat.h>
+#include <omp.h>
 
+#include <algorithm>
 #include <cfloat>
 #include <memory>
 #include <string>
@@ -150,7 +152,9 @@ struct RowSpan {
     int first[kBox], last[kBox];
 };
 
-void fill_triangle(BoxRaster &R, float diffuse, float z, const V2 &v1, const V2 &v2, const V2 &v3, RowSpan &span) {
+// Sample rows rlo..rhi-1 only (one thread's band).
+void fill_triangle(BoxRaster &R, float diffuse, float z, const V2 &v1, const V2 &v2, const V2 &v3, RowSpan &span,
+                   int rlo, int rhi) {
     const float fxmin = fminf(v1.x, fminf(v2.x, v3.x));
     const float fymin = fminf(v1.y, fminf(v2.y, v3.y));
     const float fxmax = fmaxf(v1.x, fmaxf(v2.x, v3.x));
@@ -166,7 +170,8 @@ void fill_triangle(BoxRaster &R, float diffuse, float z, const V2 &v1, const V2 
     if (gx0 > xmax || gx0 >= kRaster || gy0 > ymax || gy0 >= kRaster) return;
     const int nw = xmax - xmin + 1, nh = ymax - ymin + 1;
     const int gy1 = ymax < kRaster - 1 ? ymax : kRaster - 1;
-    const int r0 = gy0 / kStride, r1 = gy1 / kStride;
+    const int r0 = std::max(gy0 / kStride, rlo), r1 = std::min(gy1 / kStride, rhi - 1);
+    if (r0 > r1) return;
     for (int r = r0; r <= r1; ++r) {
         span.first[r] = nw;
         span.last[r] = -1;
@@ -175,7 +180,7 @@ void fill_triangle(BoxRaster &R, float diffuse, float z, const V2 &v1, const V2 
     auto dot = [&](int x, int y) {
         if (y < 0 || y >= nh || x < 0 || x >= nw) return;
         const int yy = y + ymin;
-        if (yy % kStride != 0 || yy < gy0 || yy > gy1) return;
+        if (yy % kStride != 0 || yy < r0 * kStride || yy > r1 * kStride) return;
         const int r = yy / kStride;
         if (x < span.first[r]) span.first[r] = x;
         if (x > span.last[r]) span.last[r] = x;
@@ -197,6 +202,21 @@ void fill_triangle(BoxRaster &R, float diffuse, float z, const V2 &v1, const V2 
         }
         (void)gy;
     }
+}
+
+// A facet after culling and projection: its diffuse term, depth, image
+// corners and the band [rlo, rhi) of sample rows its box reaches (empty
+// when culled or missing every sample).
+struct Shaded {
+    float d, z;
+    V2 v1, v2, v3;
+    int rlo, rhi;
+};
+
+// Host threads for the overlay: all the process may use, at most 16.
+int overlay_threads() {
+    const int n = omp_get_max_threads();
+    return n < 1 ? 1 : (n > 16 ? 16 : n);
 }
 
 void set_err(const std::string &m) { mk::set_last_error(m); }
@@ -308,33 +328,84 @@ extern "C" int mk_merge_orientation_box(mk_mesh mesh, const float rotate[9], uin
     if (width <= kBox || height <= kBox) return MK_OK;   // MonkeyGL draws no box on small images
     std::unique_ptr<BoxRaster> R(new BoxRaster);
     memset(R.get(), 0, sizeof(BoxRaster));
-    RowSpan span;
     float m[9];
     memcpy(m, rotate, sizeof(m));
-    std::vector<V3> rv(mesh->verts.size());
-    for (size_t i = 0; i < rv.size(); ++i) rv[i] = rotate_point(m, mesh->verts[i]);
+    const size_t nv = mesh->verts.size(), nf = mesh->tri.size() / 3;
+    std::vector<V3> rv(nv);
+    std::vector<Shaded> sf(nf);
     const V3 view = direction(0.0f, -1.0f, 0.0f);
-    const size_t nf = mesh->tri.size() / 3;
-    for (size_t f = 0; f < nf; ++f) {
-        // VRImageLayer::GetMeshPoints (core/VRImageLayer.cpp:166-194)
-        const V3 &a = rv[mesh->tri[3 * f]], &b = rv[mesh->tri[3 * f + 1]], &c = rv[mesh->tri[3 * f + 2]];
-        const V3 e1 = direction_from(c, a), e2 = direction_from(c, b);
-        const float cx = e1.y * e2.z - e1.z * e2.y;
-        const float cy = e1.z * e2.x - e1.x * e2.z;
-        const float cz = e1.x * e2.y - e1.y * e2.x;
-        // N.(0,-1,0) < 0 exactly when the unnormalised cross product points
-        // along +y (its length is then positive), so those facets go before
-        // the normalisation
-        if (cy > 0) continue;
-        const V3 n = direction(cx, cy, cz);
-        float d = 0;
-        d += n.x * view.x;
-        d += n.y * view.y;
-        d += n.z * view.z;
-        if (d < 0) continue;
-        const float z = (a.y + b.y + c.y) / 3 + 10000;
-        fill_triangle(*R, d, z, to_image(a.x, a.z, kRaster, kRaster), to_image(b.x, b.z, kRaster, kRaster),
-                      to_image(c.x, c.z, kRaster, kRaster), span);
+    const int nthreads = overlay_threads();
+    // phase 1, over vertices and then facets: turn, cull and project
+    // (VRImageLayer::GetMeshPoints, core/VRImageLayer.cpp:166-194)
+#pragma omp parallel num_threads(nthreads)
+    {
+#pragma omp for schedule(static)
+        for (long i = 0; i < (long)nv; ++i) rv[i] = rotate_point(m, mesh->verts[i]);
+#pragma omp for schedule(static)
+        for (long f = 0; f < (long)nf; ++f) {
+            Shaded &o = sf[f];
+            o.rlo = 1;
+            o.rhi = 0;   // empty: culled or no sample point
+            const V3 &a = rv[mesh->tri[3 * f]], &b = rv[mesh->tri[3 * f + 1]], &c = rv[mesh->tri[3 * f + 2]];
+            const V3 e1 = direction_from(c, a), e2 = direction_from(c, b);
+            const float cx = e1.y * e2.z - e1.z * e2.y;
+            const float cy = e1.z * e2.x - e1.x * e2.z;
+            const float cz = e1.x * e2.y - e1.y * e2.x;
+            // N.(0,-1,0) < 0 exactly when the unnormalised cross product
+            // points along +y (its length is then positive), so those
+            // facets go before the normalisation
+            if (cy > 0) continue;
+            const V3 n = direction(cx, cy, cz);
+            float d = 0;
+            d += n.x * view.x;
+            d += n.y * view.y;
+            d += n.z * view.z;
+            if (d < 0) continue;
+            o.d = d;
+            o.z = (a.y + b.y + c.y) / 3 + 10000;
+            o.v1 = to_image(a.x, a.z, kRaster, kRaster);
+            o.v2 = to_image(b.x, b.z, kRaster, kRaster);
+            o.v3 = to_image(c.x, c.z, kRaster, kRaster);
+            // sample rows its bounding box reaches (fill_triangle's own test)
+            const float fymin = fminf(o.v1.y, fminf(o.v2.y, o.v3.y));
+            const float fymax = fmaxf(o.v1.y, fmaxf(o.v2.y, o.v3.y));
+            const int ymin = int(fymin), ymax = int(fymax + 0.5);
+            if (ymin >= kRaster || ymax < 0) continue;
+            const int gy0 = ymin <= 0 ? 0 : (ymin + kStride - 1) / kStride * kStride;
+            const int gy1 = ymax < kRaster - 1 ? ymax : kRaster - 1;
+            if (gy0 > gy1) continue;
+            o.rlo = gy0 / kStride;
+            o.rhi = gy1 / kStride + 1;
+        }
+    }
+    // phase 2, over bands of sample rows holding about equal numbers of
+    // facets: every band takes its facets in mesh order, so each sample
+    // sees MonkeyGL's z-buffer sequence
+    int band[17];
+    {
+        long hist[kBox] = {}, total = 0;
+        for (size_t f = 0; f < nf; ++f)
+            for (int r = sf[f].rlo; r < sf[f].rhi; ++r) ++hist[r];
+        for (int r = 0; r < kBox; ++r) total += hist[r];
+        band[0] = 0;
+        long acc = 0;
+        int b = 1;
+        for (int r = 0; r < kBox && b < nthreads; ++r) {
+            acc += hist[r];
+            if (acc * nthreads >= total * b) band[b++] = r + 1;
+        }
+        for (; b <= nthreads; ++b) band[b] = kBox;
+    }
+#pragma omp parallel num_threads(nthreads)
+    {
+        const int t = omp_get_thread_num();
+        const int blo = t < nthreads ? band[t] : kBox, bhi = t < nthreads ? band[t + 1] : kBox;
+        RowSpan span;
+        for (size_t f = 0; f < nf && blo < bhi; ++f) {
+            const Shaded &o = sf[f];
+            if (o.rhi <= blo || o.rlo >= bhi) continue;
+            fill_triangle(*R, o.d, o.z, o.v1, o.v2, o.v3, span, blo, bhi);
+        }
     }
     // VRImageLayer::MergeOrientationBox: RGBA(0.902, 0.902, 0.302) * diffuse
     // + 0.05, each step clamped to [0, 1], truncated to 8 bits

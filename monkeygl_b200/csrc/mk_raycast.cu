@@ -153,7 +153,7 @@ __global__ void k_fy_table(const float *__restrict__ accu, int n, float scale, f
 // The fy table of volume v at `scale`, cached on the volume (8 scales).  A
 // new table is built on `s` and waited for once, so launches on other
 // streams can share it.
-static int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out) {
+int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out) {
     for (int i = 0; i < v.n_fy_tables; ++i) {
         if (memcmp(&v.fy_tables[i].scale, &scale, sizeof(float)) == 0) {
             *out = v.fy_tables[i].d_fy;

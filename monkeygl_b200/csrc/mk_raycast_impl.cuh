@@ -82,10 +82,11 @@ __device__ __forceinline__ float3 ray_pos(const RayParams &P, float u, float v, 
     return ray_pos_fy(P, u, v, ray_fy(a, P.scale));
 }
 
-// The position of a sample that lies on the schedule table (a == accu[k]):
-// its ray parameter comes from the frame's table when there is one.
+// The position of a sample that lies on the schedule table (a == accu[k]).
+// Rendering launches carry the frame's fy table; counting passes evaluate.
+template <bool COUNT>
 __device__ __forceinline__ float3 ray_pos_at(const RayParams &P, float u, float v, int k, float a) {
-    return P.fy_tab ? ray_pos_fy(P, u, v, P.fy_tab[k]) : ray_pos(P, u, v, a);
+    return COUNT ? ray_pos(P, u, v, a) : ray_pos_fy(P, u, v, P.fy_tab[k]);
 }
 
 // Interval [a0, a1] of accuLength where the ray may touch the VOI, from the
@@ -457,7 +458,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                 if (!(aj < P.limit) || aj > Q.a_stop) {
                     flags = kCoopEnd;
                 } else {
-                    const float3 pos = kj >= 0 ? ray_pos_at(P, Q.u, Q.v, kj, aj) : ray_pos(P, Q.u, Q.v, aj);
+                    const float3 pos = kj >= 0 ? ray_pos_at<false>(P, Q.u, Q.v, kj, aj) : ray_pos(P, Q.u, Q.v, aj);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
@@ -648,7 +649,7 @@ __device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject
                 R.done = true;
                 break;
             }
-            const float3 pos = R.lat >= 0 ? ray_pos_at(P, R.u, R.v, R.lat, R.a) : ray_pos(P, R.u, R.v, R.a);
+            const float3 pos = R.lat >= 0 ? ray_pos_at<false>(P, R.u, R.v, R.lat, R.a) : ray_pos(P, R.u, R.v, R.a);
             const int ix = pos.x * P.fdim[0];
             const int iy = pos.y * P.fdim[1];
             const int iz = pos.z * P.fdim[2];
@@ -818,7 +819,7 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                 int k = k0;
                 while (a < P.limit) {
                     if (a > a_stop) break;
-                    const float3 pos = ray_pos_at(P, u, v, k, a);
+                    const float3 pos = ray_pos_at<COUNT>(P, u, v, k, a);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
@@ -868,7 +869,7 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                 int k = k0;
                 while (a < P.limit) {
                     if (a > a_stop) break;
-                    const float3 pos = ray_pos_at(P, u, v, k, a);
+                    const float3 pos = ray_pos_at<COUNT>(P, u, v, k, a);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
@@ -971,6 +972,9 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
 // pointer is left null), and the opacity-accumulator mode for the labels
 // present in a volume under a table of (alpha, ww, wl) rows.
 int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P);
+// Host: the ray parameter of every schedule entry at `scale` (cached on the
+// volume); rendering kernels read it for the samples on the table.
+int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out);
 int tracking_mode_for(const uint64_t present[2], const float (*params)[3]);
 // Host: the 32x8 tiles of a W x H frame (index by * tiles_x + bx) sorted by
 // the distance of their centre to (W/2 + xT, H/2 + yT), where the volume

@@ -292,6 +292,8 @@ int admit(mk_server_s *s, uint64_t ticket, int slot_index) {
         D.mode = q.r.kind;
         fill_ray_params(vs, &vp, D.rp);
         D.rp.out = static_cast<uint8_t *>(sl.d_out);
+        int trc = fy_table(vs, D.rp.scale, s->stream, &D.rp.fy_tab);
+        if (trc != MK_OK) return trc;
         float params[MK_MAX_LABELS][3];
         for (int l = 0; l < MK_MAX_LABELS; ++l) {
             const bool has = l < q.r.n_luts;

@@ -9,7 +9,9 @@ Rows (synthetic seeded phantoms of monkeygl_b200.phantom):
   * CPR of a cardiac vessel, 1024 rows x 512 columns, stretched and
     straightened;
   * differentiable VR: float32 256^3 volume, 256-entry LUT, 8 views of 256^2,
-    step 0.5 voxel -- forward, backward and their ratio.
+    step 0.5 voxel -- forward, backward and their ratio;
+  * GetVRData through the HelloMonkey API (render, orientation box, copy
+    back), 512x512, 36 views, beside MonkeyGL's complete HelloMonkey path.
 
 Device times are CUDA events on the launching stream around each call, L2
 flushed (256 MiB write) between calls outside the events, median over the
@@ -240,14 +242,82 @@ def dvr_rows(ctx):
              "bwd_over_fwd": round(b / f, 3), "gsamples_per_s": round(samples / b / 1e6, 2)}]
 
 
-def main(args=None, ref=None):
+def api_rows(ctx):
+    """GetVRData through the drop-in API (render, orientation box, copy back)
+    against MonkeyGL's complete HelloMonkey path on the same calls: the
+    cardiac phantom, a 100-entry TF from 4 control points, window 1700/650,
+    512x512 VR (MonkeyGL's default size), 36 views 10 degrees apart.  Both
+    objects are made in the directory holding resources/human.stl, so both
+    draw the orientation box.  Wall time per call, median."""
+    import os
+    import sys
+    from pathlib import Path
+    lib = Path(__file__).resolve().parent / "lib"
+    if str(lib) not in sys.path:
+        sys.path.insert(0, str(lib))
+    import pyMonkeyGL as pm
+    ref = ctx.get("ref_api")
+    w = _workload(ctx, "cardiac")
+    vol = w.phantom.volume
+    tf = {0: (0.9, 0.3, 0.2, 0.0), 22: (0.95, 0.4, 0.3, 0.0), 55: (0.9, 0.7, 0.5, 0.35), 99: (1.0, 0.95, 0.9, 0.85)}
+    cwd = os.getcwd()
+    res_dir = ctx.get("resources_dir")
+    if res_dir:
+        os.chdir(res_dir)
+    try:
+        mine = pm.HelloMonkey()
+    finally:
+        os.chdir(cwd)
+    mine.SetVolumeArray(vol.swapaxes(2, 0))
+    mine.SetDirection(pm.Direction3d(1, 0, 0), pm.Direction3d(0, 1, 0), pm.Direction3d(0, 0, -1))
+    mine.SetSpacing(*w.spacing)
+    mine.SetTransferFunc({k: pm.RGBA(*v) for k, v in tf.items()})
+    mine.SetVRWWWL(1700.0, 650.0)
+    mine.SetVRSize(512, 512)
+    mine.Anterior()
+    times, same = [], True
+    if ref is not None:
+        ref.set_volume(vol, w.spacing)
+        ref.set_transfer_function(tf)
+        ref.set_wwwl(1700.0, 650.0)
+        ref.set_vr_size(512, 512)
+        ref.orientation(0)
+    for i in range(3):
+        mine.GetVRImage()
+        if ref is not None:
+            ref.vr_image()
+    rtimes = []
+    for i in range(36):
+        mine.Rotate(10.0, 0.0)
+        t0 = time.perf_counter()
+        img = mine.GetVRImage()
+        times.append((time.perf_counter() - t0) * 1e3)
+        if ref is not None:
+            ref.rotate(10.0, 0.0)
+            t0 = time.perf_counter()
+            rimg = ref.vr_image()
+            rtimes.append((time.perf_counter() - t0) * 1e3)
+            same = same and np.array_equal(img, rimg)
+    ms = statistics.median(times)
+    row = {"row": "GetVRData cardiac 512^2 (API: render + orientation box + copy)", "image": "512x512",
+           "e2e_ms": round(ms, 4), "fps": round(1e3 / ms, 1)}
+    if ref is not None:
+        rms = statistics.median(rtimes)
+        row.update({"ref_call_ms": round(rms, 4), "speedup_e2e": round(rms / ms, 2), "identical_images": same})
+    return [row]
+
+
+def main(args=None, ref=None, ref_api=None, resources_dir=None):
     """Print the table.  `ref` is MonkeyGL's own CUDA path (an object with
     set_volume / set_mask / clear_tfs / set_lut / kernel_ms / plane / cpr),
-    supplied by the caller, or None for no reference columns."""
+    `ref_api` its complete HelloMonkey (set_volume / set_transfer_function /
+    set_wwwl / set_vr_size / orientation / rotate / vr_image) and
+    `resources_dir` the directory holding resources/human.stl, all supplied
+    by the caller, or None for no reference columns."""
     import torch
     torch.cuda.init()
     ctx = {"stream": torch.cuda.Stream(), "flush": torch.empty(256 << 20, dtype=torch.uint8, device="cuda"),
-           "ref": ref}
+           "ref": ref, "ref_api": ref_api, "resources_dir": resources_dir}
     only = {g for g in (getattr(args, "suite_only", "") or "").split(",") if g}
     want = lambda g: not only or g in only
     rows = []
@@ -261,6 +331,8 @@ def main(args=None, ref=None):
         rows += cpr_rows(ctx)
     if want("dvr"):
         rows += dvr_rows(ctx)
+    if want("api"):
+        rows += api_rows(ctx)
     for r in rows:
         print(json.dumps(r), flush=True)
     keys = ["row", "image", "ms", "e2e_ms", "ref_kernel_ms", "ref_call_ms", "speedup_kernel", "speedup_e2e",

@@ -210,3 +210,77 @@ class RefGPU:
         out = np.zeros((h, w), np.int16)
         assert self.L.mkref_cpr(_vp(out), w, h, _vp(pts), _vp(dirs), int(bool(invert_z))) == 0
         return out
+
+
+REF_FULL_LIB = HERE / "_ref" / "libmkref_full.so"
+
+
+def ref_full_available() -> bool:
+    return REF_FULL_LIB.exists() and (HERE / "_ref" / "resources" / "human.stl").exists()
+
+
+class RefHelloMonkey:
+    """MonkeyGL's complete HelloMonkey (its host code and kernels, built
+    unmodified into _ref/libmkref_full.so), driven through the mkrh_*
+    functions of ref_host_capture.cpp.  MonkeyGL keeps one process-wide
+    state, so every instance drives the same singleton."""
+
+    _L = None
+    _h = None
+
+    def __init__(self):
+        if RefHelloMonkey._L is None:
+            if not ref_full_available():
+                raise FileNotFoundError(f"{REF_FULL_LIB} missing; run `make -C oracle ref`")
+            L = C.CDLL(str(REF_FULL_LIB))
+            vp = C.c_void_p
+            L.mkrh_create.restype = vp
+            L.mkrh_create.argtypes = [C.c_char_p]
+            for f, a in {
+                "mkrh_set_volume": [vp, vp, C.c_int, C.c_int, C.c_int], "mkrh_set_spacing": [vp, C.c_double,
+                                                                                              C.c_double, C.c_double],
+                "mkrh_set_direction": [vp, vp], "mkrh_set_wwwl": [vp, C.c_float, C.c_float, C.c_int],
+                "mkrh_orientation": [vp, C.c_int], "mkrh_rotate": [vp, C.c_float, C.c_float],
+                "mkrh_set_vr_size": [vp, C.c_int, C.c_int], "mkrh_vr_image": [vp, vp, C.c_longlong, vp],
+                "mkrh_set_tf": [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int],
+                "mkrh_set_cpr_line_voxel": [vp, vp, C.c_int],
+            }.items():
+                getattr(L, f).argtypes = a
+            assert L.mkrh_zero_heap(1) == 1
+            RefHelloMonkey._L = L
+            RefHelloMonkey._h = L.mkrh_create(str(REF_FULL_LIB.parent).encode())
+        self.L, self.h = RefHelloMonkey._L, RefHelloMonkey._h
+        self.L.mkrh_set_cpr_line_voxel(self.h, _vp(np.zeros((1, 3))), 0)
+        self._img = np.zeros(4096 * 4096 * 3, np.uint8)
+
+    def set_volume(self, vox, spacing, direction=(1, 0, 0, 0, 1, 0, 0, 0, -1)):
+        self.vox = np.ascontiguousarray(vox, np.int16)
+        Z, Y, X = self.vox.shape
+        self.L.mkrh_set_volume(self.h, _vp(self.vox), X, Y, Z)
+        self.L.mkrh_set_direction(self.h, _vp(np.asarray(direction, np.float64)))
+        self.L.mkrh_set_spacing(self.h, *[float(s) for s in spacing])
+
+    def set_transfer_function(self, points, label=-1):
+        """points: {position 0..99: (r, g, b, a)}"""
+        pos = np.array(list(points), np.int32)
+        val = np.array([points[k] for k in points], np.float32)
+        z = np.zeros(1, np.int32)
+        return self.L.mkrh_set_tf(self.h, _vp(pos), _vp(val), len(pos), _vp(z), _vp(z.astype(np.float32)), 0, label)
+
+    def set_wwwl(self, ww, wl, label=-1):
+        return self.L.mkrh_set_wwwl(self.h, ww, wl, label)
+
+    def orientation(self, which):
+        self.L.mkrh_orientation(self.h, which)
+
+    def rotate(self, fx, fy):
+        self.L.mkrh_rotate(self.h, fx, fy)
+
+    def set_vr_size(self, w, h):
+        return self.L.mkrh_set_vr_size(self.h, w, h)
+
+    def vr_image(self):
+        wh = np.zeros(2, np.int32)
+        assert self.L.mkrh_vr_image(self.h, _vp(self._img), self._img.size, _vp(wh)) == 1
+        w, h = int(wh[0]), int(wh[1])
+        return self._img[: w * h * 3].reshape(h, w, 3)
