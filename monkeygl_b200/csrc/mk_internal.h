@@ -94,9 +94,15 @@ struct VolumeState {
     struct FyTable {
         float scale;
         float *d_fy;
+        cudaEvent_t ready;      // recorded after the table is built
+        cudaEvent_t last_use;   // recorded after the last launch that read it
+        cudaStream_t user;      // stream of the launches that read it
+        bool shared;            // read from more than one stream
+        uint64_t stamp;         // last use (least recently used is replaced)
     };
     FyTable fy_tables[8] = {};
     int n_fy_tables = 0;
+    uint64_t fy_clock = 0;
 
     size_t device_bytes = 0;
 };

@@ -150,34 +150,63 @@ __global__ void k_fy_table(const float *__restrict__ accu, int n, float scale, f
     if (i < n) out[i] = ray_fy(accu[i], scale);
 }
 
+int launch_fy_table(const VolumeState &v, float scale, float *out, cudaStream_t s) {
+    k_fy_table<<<(v.accu_len + 255) / 256, 256, 0, s>>>(v.d_accu, v.accu_len, scale, out);
+    MK_CUDA_TRY(cudaGetLastError());
+    return MK_OK;
+}
+
 // The fy table of volume v at `scale`, cached on the volume (8 scales).  A
-// new table is built on `s` and waited for once, so launches on other
-// streams can share it.
-int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out) {
+// new table is built on `s` without waiting: launches on `s` follow it in
+// stream order, and a launch on another stream that finds it in the cache
+// waits for its `ready` event.  The caller records `*used` on its stream after
+// the launch that reads the table; replacing the least recently used table (a
+// ninth scale) waits on the host for that event, or for the whole device when
+// the table was read from more than one stream.
+int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, cudaEvent_t *used) {
     for (int i = 0; i < v.n_fy_tables; ++i) {
-        if (memcmp(&v.fy_tables[i].scale, &scale, sizeof(float)) == 0) {
-            *out = v.fy_tables[i].d_fy;
+        VolumeState::FyTable &t = v.fy_tables[i];
+        if (memcmp(&t.scale, &scale, sizeof(float)) == 0) {
+            MK_CUDA_TRY(cudaStreamWaitEvent(s, t.ready, 0));
+            t.shared |= s != t.user;
+            t.stamp = ++v.fy_clock;
+            *out = t.d_fy;
+            *used = t.last_use;
             return MK_OK;
         }
     }
-    if (v.n_fy_tables == 8) {   // drop the oldest
-        MK_CUDA_TRY(cudaStreamSynchronize(s));
-        cudaFree(v.fy_tables[0].d_fy);
-        for (int i = 1; i < 8; ++i) v.fy_tables[i - 1] = v.fy_tables[i];
-        v.n_fy_tables = 7;
+    int i = v.n_fy_tables;
+    if (i == 8) {
+        i = 0;
+        for (int j = 1; j < 8; ++j)
+            if (v.fy_tables[j].stamp < v.fy_tables[i].stamp) i = j;
+        if (v.fy_tables[i].shared) {
+            MK_CUDA_TRY(cudaDeviceSynchronize());
+        } else {
+            MK_CUDA_TRY(cudaEventSynchronize(v.fy_tables[i].last_use));
+        }
+    } else {
+        VolumeState::FyTable t = {};
+        MK_CUDA_TRY(cudaMalloc(&t.d_fy, (size_t)v.accu_len * sizeof(float)));
+        if (cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&t.last_use, cudaEventDisableTiming) != cudaSuccess) {
+            if (t.ready) cudaEventDestroy(t.ready);
+            cudaFree(t.d_fy);
+            set_last_error("fy table: event creation failed");
+            return MK_ERR_CUDA;
+        }
+        v.fy_tables[v.n_fy_tables++] = t;
     }
-    float *d = nullptr;
-    MK_CUDA_TRY(cudaMalloc(&d, (size_t)v.accu_len * sizeof(float)));
-    k_fy_table<<<(v.accu_len + 255) / 256, 256, 0, s>>>(v.d_accu, v.accu_len, scale, d);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        cudaFree(d);
-        set_last_error(std::string("fy table: ") + cudaGetErrorString(e));
-        return MK_ERR_CUDA;
-    }
-    v.fy_tables[v.n_fy_tables++] = {scale, d};
-    *out = d;
+    VolumeState::FyTable &t = v.fy_tables[i];
+    int rc = launch_fy_table(v, scale, t.d_fy, s);
+    if (rc != MK_OK) return rc;
+    MK_CUDA_TRY(cudaEventRecord(t.ready, s));
+    t.scale = scale;
+    t.user = s;
+    t.shared = false;
+    t.stamp = ++v.fy_clock;
+    *out = t.d_fy;
+    *used = t.last_use;
     return MK_OK;
 }
 
@@ -274,11 +303,13 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     const int *order = nullptr;
     rc = tile_order(v, P, s, &order);
     if (rc != MK_OK) return rc;
-    rc = fy_table(v, P.scale, s, &P.fy_tab);
+    cudaEvent_t fy_used = nullptr;
+    rc = fy_table(v, P.scale, s, &P.fy_tab, &fy_used);
     if (rc != MK_OK) return rc;
     launch_raycast<false>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
                           label_table(&v), brick_view(&v), order, s);
     MK_CUDA_TRY(cudaGetLastError());
+    MK_CUDA_TRY(cudaEventRecord(fy_used, s));
     return finish_output(&v, out, bytes, out_on_device, s);
 }
 

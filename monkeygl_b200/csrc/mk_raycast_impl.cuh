@@ -974,7 +974,10 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
 int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P);
 // Host: the ray parameter of every schedule entry at `scale` (cached on the
 // volume); rendering kernels read it for the samples on the table.
-int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out);
+// The caller records *used on s after its launch that reads the table.
+int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, cudaEvent_t *used);
+// Host: build that table into `out` (v.accu_len floats) on stream s.
+int launch_fy_table(const VolumeState &v, float scale, float *out, cudaStream_t s);
 int tracking_mode_for(const uint64_t present[2], const float (*params)[3]);
 // Host: the 32x8 tiles of a W x H frame (index by * tiles_x + bx) sorted by
 // the distance of their centre to (W/2 + xT, H/2 + yT), where the volume

@@ -141,6 +141,8 @@ struct Slot {
     void *h_stage = nullptr;            // pinned output staging
     float *h_lut = nullptr;             // pinned LUT staging (max_labels * lut_len * 4)
     float *h_alpha = nullptr;           // pinned alpha staging (max_labels * lut_len)
+    float *d_fy = nullptr;              // ray parameter table of the request (grown on demand)
+    int fy_cap = 0;
     uint64_t ticket = 0;                // 0 = free
 };
 
@@ -238,6 +240,7 @@ void release(mk_server_s *s) {
         cudaFree(sl.d_vis);
         cudaFree(sl.d_tmax);
         cudaFree(sl.d_out);
+        cudaFree(sl.d_fy);
         cudaFreeHost(sl.h_stage);
         cudaFreeHost(sl.h_lut);
         cudaFreeHost(sl.h_alpha);
@@ -292,8 +295,19 @@ int admit(mk_server_s *s, uint64_t ticket, int slot_index) {
         D.mode = q.r.kind;
         fill_ray_params(vs, &vp, D.rp);
         D.rp.out = static_cast<uint8_t *>(sl.d_out);
-        int trc = fy_table(vs, D.rp.scale, s->stream, &D.rp.fy_tab);
+        // the slot's own table, built on the admission stream like its brick
+        // maps (the slot's previous request, and with it every kernel that
+        // read the old table, has finished)
+        if (sl.fy_cap < vs.accu_len) {
+            cudaFree(sl.d_fy);
+            sl.d_fy = nullptr;
+            sl.fy_cap = 0;
+            MK_CUDA_TRY(cudaMalloc(&sl.d_fy, (size_t)vs.accu_len * sizeof(float)));
+            sl.fy_cap = vs.accu_len;
+        }
+        int trc = launch_fy_table(vs, D.rp.scale, sl.d_fy, s->stream);
         if (trc != MK_OK) return trc;
+        D.rp.fy_tab = sl.d_fy;
         float params[MK_MAX_LABELS][3];
         for (int l = 0; l < MK_MAX_LABELS; ++l) {
             const bool has = l < q.r.n_luts;
