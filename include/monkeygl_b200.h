@@ -76,7 +76,8 @@ typedef enum mk_pixel_format {
 
 /* mk_vr_params.flags */
 #define MK_VR_NO_SKIP 0x1 /* march every reference sample (no empty-space skipping) */
-#define MK_VR_NO_COOP 0x2 /* VR: one lane per ray to the end (no cooperative tail; same image) */
+#define MK_VR_NO_COOP 0x2 /* VR: one lane per ray to the end (no cooperative tail, no tail launch; same image) */
+#define MK_VR_NO_TAIL 0x4 /* VR: no tail launch (rays finish in the tile launch; same image) */
 
 typedef struct mk_volume_s *mk_volume;
 

@@ -35,6 +35,7 @@ SAMPLE_LINEAR, SAMPLE_NEAREST = 0, 1
 PIXEL_RGB8, PIXEL_RGBA8 = 0, 1
 VR_NO_SKIP = 0x1
 VR_NO_COOP = 0x2
+VR_NO_TAIL = 0x4
 
 
 class MonkeyGLError(RuntimeError):

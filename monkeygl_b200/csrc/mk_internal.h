@@ -104,6 +104,18 @@ struct VolumeState {
     int n_fy_tables = 0;
     uint64_t fy_clock = 0;
 
+    // VR frame tail: counters and spill list, one set per rendering stream
+    // (the tile launch and the tail launch of a frame use them in stream
+    // order; the tail launch leaves the counters at zero)
+    struct TailBuf {
+        cudaStream_t stream;
+        unsigned *d_tail;       // 4 counters
+        void *d_rays;           // spill list
+        int cap;                // rays it holds
+    };
+    TailBuf tails[4] = {};
+    int n_tails = 0;
+
     size_t device_bytes = 0;
 };
 

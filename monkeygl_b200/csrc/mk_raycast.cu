@@ -36,6 +36,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -71,6 +72,88 @@ __global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_
         by = t / tx;
     }
     raycast_tile<MODE, TRACK, COUNT>(P, vol, mask, S, BV, s_acc, s_coop, s_px, &s_count, bx, by);
+    if (MODE == kModeVR && !COUNT && P.tail) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(&P.tail[0], 1u);
+    }
+}
+
+// The tail launch of a VR frame: resumes the rays that the tile launch
+// spilled (same P, same tables) with as many lanes per ray as the grid
+// allows (vr_coop_tail: groups of 32 / rays-per-warp lanes), writes their
+// pixels, and resets the frame's tail counters for the next frame.
+template <int TRACK>
+__global__ void __launch_bounds__(256) k_vr_tail(RayParams P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+                                                 LabelTable LT, BrickView BV) {
+    __shared__ LabelSmem S;
+    __shared__ float s_acc[TRACK == kTrackShared ? kMaxTrackedLabels : 1][256];
+    __shared__ CoopSample s_coop[256];
+    __shared__ unsigned s_n;
+    load_label_smem(S, LT, TRACK);
+    if (threadIdx.x == 0) s_n = min(*(volatile unsigned *)&P.tail[1], (unsigned)P.spill_cap);
+    __syncthreads();
+    const unsigned n = s_n;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const unsigned warps = gridDim.x * (blockDim.x / 32);
+    unsigned per = 1;          // rays per warp: a power of two, at most 32
+    while (per < 32 && per * warps < n) per <<= 1;
+    const StepVec dv = step_vec(P);
+    const float3 L = vr_light(P);
+    while (true) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(&P.tail[2], per);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const unsigned cnt = min(per, n - base);
+        VrRay R;
+        R.done = true;
+        R.sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if ((unsigned)lane < cnt) {
+            const SpillRay &q = P.spill[base + lane];
+            R.sum = q.sum;
+            R.u = q.u;
+            R.v = q.v;
+            R.a = q.a;
+            R.a_stop = q.a_stop;
+            R.step = q.step;
+            R.aPre = q.aPre;
+            R.A = q.A;
+            R.lat = q.lat;
+            R.pix = q.pix;
+            R.done = false;
+            if (TRACK == kTrackShared) {
+#pragma unroll
+                for (int k = 0; k < kMaxTrackedLabels; ++k) s_acc[k][tid] = q.acc[k];
+            }
+        }
+        const unsigned act = __ballot_sync(0xffffffffu, (unsigned)lane < cnt);
+        __syncwarp();
+        vr_coop_tail<TRACK>(P, vol, mask, S, BV, s_acc, s_coop + (tid & ~31), act, R, dv, L, false);
+        if ((unsigned)lane < cnt) {
+            float4 sum = R.sum;
+            if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;
+            const uint32_t rgb = pack_rgb(sum);
+            if (P.rgba) {
+                reinterpret_cast<uint32_t *>(P.out)[R.pix] = rgb | 0xff000000u;
+            } else {
+                uint8_t *o = P.out + (size_t)R.pix * 3;
+                o[0] = rgb & 0xff;
+                o[1] = (rgb >> 8) & 0xff;
+                o[2] = (rgb >> 16) & 0xff;
+            }
+        }
+    }
+    // the last block to finish resets the counters for the next frame
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&P.tail[3], 1u) == gridDim.x - 1) {
+            P.tail[0] = 0;
+            P.tail[1] = 0;
+            P.tail[2] = 0;
+            P.tail[3] = 0;
+        }
+    }
 }
 
 template <int MODE, int TRACK, bool COUNT>
@@ -94,6 +177,76 @@ static void launch_raycast(int mode, int track, const RayParams &P, cudaTextureO
     } else {
         launch_mode<kModeSurface, kTrackNone, COUNT>(P, vol, mask, LT, BV, order, s);
     }
+}
+
+// Tiles still unfinished when rays start to spill to the tail launch
+// (MONKEYGL_B200_TAIL_TILES overrides it; 0 spills from the first check).
+static int tail_tiles() {
+    static const int k = [] {
+        const char *e = getenv("MONKEYGL_B200_TAIL_TILES");
+        return e ? std::max(0, atoi(e)) : 296;
+    }();
+    return k;
+}
+
+// The tail buffers of stream s (created on first use, grown for larger
+// frames) and the frame's tail fields of P.  Four streams per volume have
+// their own; a fifth renders without a tail launch.
+static int tail_params(VolumeState &v, RayParams &P, cudaStream_t s) {
+    const int ntiles = ((P.W + 31) / 32) * ((P.H + 7) / 8);
+    const int K = tail_tiles();
+    const int want = (int)std::min<long long>((long long)P.W * P.H, std::max(4LL * K * 256, 65536LL));
+    int i = 0;
+    while (i < v.n_tails && v.tails[i].stream != s) ++i;
+    if (i == v.n_tails) {
+        if (v.n_tails == 4) return MK_OK;
+        VolumeState::TailBuf t = {};
+        t.stream = s;
+        MK_CUDA_TRY(cudaMalloc(&t.d_tail, 4 * sizeof(unsigned)));
+        if (cudaMemsetAsync(t.d_tail, 0, 4 * sizeof(unsigned), s) != cudaSuccess) {
+            cudaFree(t.d_tail);
+            set_last_error("tail counters: memset failed");
+            return MK_ERR_CUDA;
+        }
+        v.tails[v.n_tails++] = t;
+    }
+    VolumeState::TailBuf &t = v.tails[i];
+    if (t.cap < want) {
+        MK_CUDA_TRY(cudaStreamSynchronize(s));     // the last frame on s is done with the list
+        cudaFree(t.d_rays);
+        t.d_rays = nullptr;
+        t.cap = 0;
+        MK_CUDA_TRY(cudaMalloc(&t.d_rays, (size_t)want * sizeof(SpillRay)));
+        t.cap = want;
+    }
+    P.tail = t.d_tail;
+    P.spill = static_cast<SpillRay *>(t.d_rays);
+    P.spill_cap = t.cap;
+    P.tail_trigger = std::max(0, ntiles - K);
+    return MK_OK;
+}
+
+template <int TRACK>
+static int launch_tail_track(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+                             const LabelTable &LT, const BrickView &BV, cudaStream_t s) {
+    static int grid = 0;
+    if (grid == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        MK_CUDA_TRY(cudaGetDevice(&dev));
+        MK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        MK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vr_tail<TRACK>, 256, 0));
+        grid = std::max(1, sms * std::max(1, per_sm));
+    }
+    k_vr_tail<TRACK><<<grid, 256, 0, s>>>(P, vol, mask, LT, BV);
+    MK_CUDA_TRY(cudaGetLastError());
+    return MK_OK;
+}
+
+static int launch_vr_tail(int track, const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+                          const LabelTable &LT, const BrickView &BV, cudaStream_t s) {
+    if (!P.tail) return MK_OK;
+    if (track == kTrackShared) return launch_tail_track<kTrackShared>(P, vol, mask, LT, BV, s);
+    return launch_tail_track<kTrackNone>(P, vol, mask, LT, BV, s);
 }
 
 std::vector<int> centre_first_tiles(int W, int H, int xT, int yT) {
@@ -271,6 +424,10 @@ int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P) {
     P.counter = nullptr;
     P.vox_bits = nullptr;
     P.lab_bits = nullptr;
+    P.tail = nullptr;
+    P.spill = nullptr;
+    P.spill_cap = 0;
+    P.tail_trigger = 0;
     return MK_OK;
 }
 
@@ -306,9 +463,20 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     cudaEvent_t fy_used = nullptr;
     rc = fy_table(v, P.scale, s, &P.fy_tab, &fy_used);
     if (rc != MK_OK) return rc;
-    launch_raycast<false>(params->render_type, tracking_mode(v), P, v.tex_linear, v.tex_mask,
-                          label_table(&v), brick_view(&v), order, s);
+    const int track = tracking_mode(v);
+    const bool tail = params->render_type == MK_RENDER_VR && track != kTrackLocal &&
+                      !(params->flags & (MK_VR_NO_TAIL | MK_VR_NO_COOP));
+    if (tail) {
+        rc = tail_params(v, P, s);
+        if (rc != MK_OK) return rc;
+    }
+    launch_raycast<false>(params->render_type, track, P, v.tex_linear, v.tex_mask, label_table(&v),
+                          brick_view(&v), order, s);
     MK_CUDA_TRY(cudaGetLastError());
+    if (tail) {
+        rc = launch_vr_tail(track, P, v.tex_linear, v.tex_mask, label_table(&v), brick_view(&v), s);
+        if (rc != MK_OK) return rc;
+    }
     MK_CUDA_TRY(cudaEventRecord(fy_used, s));
     return finish_output(&v, out, bytes, out_on_device, s);
 }

@@ -18,6 +18,19 @@ namespace mk {
 enum RayMode { kModeVR = 0, kModeMIP = 1, kModeSurface = 2 };
 enum Track { kTrackNone = 0, kTrackShared = 1, kTrackLocal = 2 };
 
+// A VR ray handed from a frame's tile launch to its tail launch: the march
+// state of MonkeyGL's loop at a sample boundary and the ray's opacity
+// accumulators, restored bit for bit by the tail launch.
+struct __align__(16) SpillRay {
+    float4 sum;
+    float u, v, a, a_stop;
+    float step, aPre, A;
+    int lat;
+    int pix;                     // y * W + x
+    int pad[3];
+    float acc[kMaxTrackedLabels];
+};
+
 struct RayParams {
     int W, H;
     float fdim[3];               // dims as float (index = trunc(pos * dim))
@@ -41,6 +54,12 @@ struct RayParams {
     unsigned long long *counter; // sample counting mode
     uint32_t *vox_bits;          // counting mode: voxels inside trilinear footprints (may be null)
     uint32_t *lab_bits;          // counting mode: label voxels read (may be null)
+    // VR frame tail (null: rays are marched to the end where they start):
+    // {tiles finished, rays spilled, rays taken, tail blocks finished}
+    unsigned *tail;
+    SpillRay *spill;             // rays handed to the tail launch
+    int spill_cap;
+    int tail_trigger;            // rays still marching spill once this many tiles have finished
 };
 
 struct LabelSmem {
@@ -376,8 +395,49 @@ struct VrRay {
     float u, v, a, a_stop, step, aPre, A;
     float4 sum;
     int lat;         // index of a in the schedule table while the step was never refined, else -1
+    int pix;         // y * W + x of the ray's pixel
     bool done;
 };
+
+// Frame tail.  Tiles of long rays set the length of a frame: near its end a
+// few warps march alone on otherwise idle SMs, at the latency of their sample
+// chains.  Once P.tail_trigger tiles have finished, a warp hands its rays that
+// are still marching to the spill list (state at a sample boundary, opacity
+// accumulators included) and stops; the tail launch (k_vr_tail) resumes them
+// with several lanes per ray on every SM.  Where a ray is handed over does
+// not change its samples or their order, so the image is unchanged.
+// Warp-uniform: lane 0 reads the finished-tile count.
+__device__ __forceinline__ bool tail_reached(const RayParams &P) {
+    unsigned t = 0;
+    if ((threadIdx.x & 31) == 0) t = *(volatile const unsigned *)P.tail;
+    t = __shfl_sync(0xffffffffu, t, 0);
+    return t >= (unsigned)P.tail_trigger;
+}
+
+// Write ray R (opacity accumulators at s_acc[.][acc_tid]) to the spill list;
+// false when the list is full (the ray then keeps marching).
+template <int TRACK>
+__device__ __forceinline__ bool spill_ray(const RayParams &P, const VrRay &R, const float (*s_acc)[256],
+                                          int acc_tid) {
+    const unsigned i = atomicAdd(&P.tail[1], 1u);
+    if (i >= (unsigned)P.spill_cap) return false;
+    SpillRay &o = P.spill[i];
+    o.sum = R.sum;
+    o.u = R.u;
+    o.v = R.v;
+    o.a = R.a;
+    o.a_stop = R.a_stop;
+    o.step = R.step;
+    o.aPre = R.aPre;
+    o.A = R.A;
+    o.lat = R.lat;
+    o.pix = R.pix;
+    if (TRACK == kTrackShared) {
+#pragma unroll
+        for (int k = 0; k < kMaxTrackedLabels; ++k) o.acc[k] = s_acc[k][acc_tid];
+    }
+    return true;
+}
 
 template <int TRACK>
 __device__ __forceinline__ bool vr_cap_ok(const LabelSmem &S, const float (*s_acc)[256], const float *accLocal,
@@ -405,7 +465,7 @@ __device__ __forceinline__ void vr_cap_add(const LabelSmem &S, float (*s_acc)[25
 template <int TRACK>
 __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
                              const LabelSmem &S, const BrickView &BV, float (*s_acc)[256], CoopSample *ws,
-                             unsigned act, VrRay &R, const StepVec &dv, float3 L) {
+                             unsigned act, VrRay &R, const StepVec &dv, float3 L, bool may_spill) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const float L1 = P.step1, L4 = L1 / 4.0f, L8 = L1 / 8.0f;
@@ -438,12 +498,14 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             T.sum.z = __shfl_sync(FULL, Q.sum.z, src);
             T.sum.w = __shfl_sync(FULL, Q.sum.w, src);
             T.lat = __shfl_sync(FULL, Q.lat, src);
+            T.pix = __shfl_sync(FULL, Q.pix, src);
             owner = __shfl_sync(FULL, owner, src);
             T.done = !member;
             Q = T;
         }
         const int owner_tid = (threadIdx.x & ~31) | owner;
         bool reported = false;
+        int round = 0;
         while (true) {
             // 1. this lane's sample, j steps ahead
             float4 clr = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -564,6 +626,16 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     ++k;
                 }
             }
+            if (may_spill && (++round & 3) == 0 && tail_reached(P)) {
+                may_spill = false;
+                bool moved = false;
+                if (member && j == 0 && !Q.done) moved = spill_ray<TRACK>(P, Q, s_acc, owner_tid);
+                moved = __shfl_sync(FULL, moved, member ? g * G : lane);
+                if (member && moved) {
+                    Q.done = true;      // finished by the tail launch: no colour from here
+                    reported = true;
+                }
+            }
             if (member && Q.done && !reported) {
                 if (j == 0) ws[owner].res = Q.sum;
                 reported = true;
@@ -585,6 +657,15 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
     __syncwarp();
 }
 
+// The headlight direction normalize(mul(M, (0,1,0))) (core/kernel.cu:166-167).
+__device__ __forceinline__ float3 vr_light(const RayParams &P) {
+    const float lx = dot3(0.0f, 1.0f, 0.0f, P.M[0], P.M[1], P.M[2]);
+    const float ly = dot3(0.0f, 1.0f, 0.0f, P.M[3], P.M[4], P.M[5]);
+    const float lz = dot3(0.0f, 1.0f, 0.0f, P.M[6], P.M[7], P.M[8]);
+    const float inv = rsqrtf(lx * lx + ly * ly + lz * lz);
+    return make_float3(lx * inv, ly * inv, lz * inv);
+}
+
 // MonkeyGL's d_render march (core/kernel.cu:156-256) for the ray of this
 // lane, called by every lane of the warp; returns the composited colour
 // (the background where nothing composited).
@@ -600,6 +681,7 @@ __device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject
     R.A = 0.0f;
     R.sum = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     R.lat = -1;
+    R.pix = y * P.W + x;
     R.done = true;
     if (active) {
         R.u = 1.0f * (x - P.W / 2.0f - P.xT) / P.H;
@@ -615,15 +697,7 @@ __device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject
         }
     }
     const StepVec dv = step_vec(P);
-    float3 L;
-    {
-        // normalize(mul(M, (0,1,0))) (core/kernel.cu:166-167)
-        float lx_ = dot3(0.0f, 1.0f, 0.0f, P.M[0], P.M[1], P.M[2]);
-        float ly_ = dot3(0.0f, 1.0f, 0.0f, P.M[3], P.M[4], P.M[5]);
-        float lz_ = dot3(0.0f, 1.0f, 0.0f, P.M[6], P.M[7], P.M[8]);
-        const float inv = rsqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_);
-        L = make_float3(lx_ * inv, ly_ * inv, lz_ * inv);
-    }
+    const float3 L = vr_light(P);
     const float L1 = P.step1;
     const float L4 = L1 / 4.0f;
     const float L8 = L1 / 8.0f;
@@ -633,78 +707,90 @@ __device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject
     } else if (TRACK == kTrackLocal) {
         for (int i = 0; i < MK_MAX_LABELS; ++i) accLocal[i] = 0.0f;
     }
+    bool may_spill = TRACK != kTrackLocal && P.tail != nullptr;
+    int iter = 0;
+    // Every lane passes the loop's votes in the same iteration: a lane whose
+    // ray is done skips only the body (no early continue), so the warp meets
+    // at one ballot per iteration.
     while (true) {
-        const unsigned act = __ballot_sync(0xffffffffu, !R.done);
+        unsigned act = __ballot_sync(0xffffffffu, !R.done);
         if (act == 0u) break;
+        if (may_spill && (++iter & 15) == 0 && tail_reached(P)) {
+            may_spill = false;
+            if (!R.done && spill_ray<TRACK>(P, R, s_acc, tid)) R.done = true;
+            act = __ballot_sync(0xffffffffu, !R.done);
+            if (act == 0u) break;
+        }
         if (TRACK != kTrackLocal && __popc(act) <= P.coop_rays) {
-            vr_coop_tail<TRACK>(P, vol, mask, S, BV, s_acc, ws + (tid & ~31), act, R, dv, L);
+            vr_coop_tail<TRACK>(P, vol, mask, S, BV, s_acc, ws + (tid & ~31), act, R, dv, L, may_spill);
             break;
         }
-        if (R.done) continue;
-        // one step of the schedule: a sample outside the VOI, a run of
-        // samples in an empty brick, or a fetched sample (lanes that take
-        // different ones diverge only within this iteration)
-        do {
-            if (!(R.a < P.limit) || R.a > R.a_stop) {
-                R.done = true;
-                break;
-            }
-            const float3 pos = R.lat >= 0 ? ray_pos_at<false>(P, R.u, R.v, R.lat, R.a) : ray_pos(P, R.u, R.v, R.a);
-            const int ix = pos.x * P.fdim[0];
-            const int iy = pos.y * P.fdim[1];
-            const int iz = pos.z * P.fdim[2];
-            if (outside_voi(P, ix, iy, iz)) {
-                R.a += R.step;
-                if (R.lat >= 0) ++R.lat;
-                break;
-            }
-            if (P.skip && R.step == L1 && R.aPre <= 0.001f) {
-                const int b = brick_index(P, BV, ix, iy, iz);
-                if (!((BV.visible_bits[b >> 5] >> (b & 31)) & 1u)) {
-                    R.aPre = 0.0f;
-                    const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1], pos.z * P.fdim[2]);
-                    advance_coarse(P, R.a, R.lat, R.step, 1 + steps_in_brick(pv, dv, ix, iy, iz));
+        if (!R.done) {
+            // one step of the schedule: a sample outside the VOI, a run of
+            // samples in an empty brick, or a fetched sample (lanes that take
+            // different ones diverge only within this iteration)
+            do {
+                if (!(R.a < P.limit) || R.a > R.a_stop) {
+                    R.done = true;
                     break;
                 }
-            }
-            const int label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
-            float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
-            temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
-            if (temp > 1) temp = 1;
-            const cudaTextureObject_t tf = S.tf[label];
-            float4 col = tf ? tex1D<float4>(tf, temp) : make_float4(0.f, 0.f, 0.f, 0.f);
-            float alpha = col.w;
-            // getNextStep (core/kernel.cu:84-125)
-            if (R.step == L4) alpha = 1 - powf(1 - alpha, 0.25f);
-            else if (R.step == L8) alpha = 1 - powf(1 - alpha, 0.125f);
-            if (R.a > 0.0f) {
-                if ((alpha > R.aPre ? alpha : R.aPre) > 0.001f) {
-                    if (R.step == L1) {
-                        R.a -= (L1 - L4);
-                        R.step = L4;
-                        R.lat = -1;
-                        break;
-                    } else if (R.step == L4) {
-                        R.a -= (L4 - L8);
-                        R.step = L8;
+                const float3 pos = R.lat >= 0 ? ray_pos_at<false>(P, R.u, R.v, R.lat, R.a) : ray_pos(P, R.u, R.v, R.a);
+                const int ix = pos.x * P.fdim[0];
+                const int iy = pos.y * P.fdim[1];
+                const int iz = pos.z * P.fdim[2];
+                if (outside_voi(P, ix, iy, iz)) {
+                    R.a += R.step;
+                    if (R.lat >= 0) ++R.lat;
+                    break;
+                }
+                if (P.skip && R.step == L1 && R.aPre <= 0.001f) {
+                    const int b = brick_index(P, BV, ix, iy, iz);
+                    if (!((BV.visible_bits[b >> 5] >> (b & 31)) & 1u)) {
+                        R.aPre = 0.0f;
+                        const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1], pos.z * P.fdim[2]);
+                        advance_coarse(P, R.a, R.lat, R.step, 1 + steps_in_brick(pv, dv, ix, iy, iz));
                         break;
                     }
-                } else {
-                    if (R.step == L8) R.step = L4;
-                    else R.step = L1;
                 }
-            }
-            R.aPre = alpha;
-            R.a += R.step;
-            if (R.lat >= 0) ++R.lat;
-            col.w = alpha;
-            if (col.w > 0.0005f && vr_cap_ok<TRACK>(S, s_acc, accLocal, label, tid)) {
-                R.sum = composite(R.sum, R.A, col.w, shade_color(vol, pos, col, L, P));
-                vr_cap_add<TRACK>(S, s_acc, accLocal, label, tid, R.A, col.w);
-                R.A += (1.0f - R.A) * col.w;
-            }
-            if (R.A > 0.995f) R.done = true;
-        } while (0);
+                const int label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
+                float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
+                temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
+                if (temp > 1) temp = 1;
+                const cudaTextureObject_t tf = S.tf[label];
+                float4 col = tf ? tex1D<float4>(tf, temp) : make_float4(0.f, 0.f, 0.f, 0.f);
+                float alpha = col.w;
+                // getNextStep (core/kernel.cu:84-125)
+                if (R.step == L4) alpha = 1 - powf(1 - alpha, 0.25f);
+                else if (R.step == L8) alpha = 1 - powf(1 - alpha, 0.125f);
+                if (R.a > 0.0f) {
+                    if ((alpha > R.aPre ? alpha : R.aPre) > 0.001f) {
+                        if (R.step == L1) {
+                            R.a -= (L1 - L4);
+                            R.step = L4;
+                            R.lat = -1;
+                            break;
+                        } else if (R.step == L4) {
+                            R.a -= (L4 - L8);
+                            R.step = L8;
+                            break;
+                        }
+                    } else {
+                        if (R.step == L8) R.step = L4;
+                        else R.step = L1;
+                    }
+                }
+                R.aPre = alpha;
+                R.a += R.step;
+                if (R.lat >= 0) ++R.lat;
+                col.w = alpha;
+                if (col.w > 0.0005f && vr_cap_ok<TRACK>(S, s_acc, accLocal, label, tid)) {
+                    R.sum = composite(R.sum, R.A, col.w, shade_color(vol, pos, col, L, P));
+                    vr_cap_add<TRACK>(S, s_acc, accLocal, label, tid, R.A, col.w);
+                    R.A += (1.0f - R.A) * col.w;
+                }
+                if (R.A > 0.995f) R.done = true;
+            } while (0);
+        }
     }
     float4 sum = R.sum;
     if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;

@@ -503,6 +503,10 @@ extern "C" int mk_volume_destroy(mk_volume v) {
     cudaFree(st.d_out);
     cudaFree(st.d_counter);
     for (int i = 0; i < st.n_orders; ++i) cudaFree(st.orders[i].d_tiles);
+    for (int i = 0; i < st.n_tails; ++i) {
+        cudaFree(st.tails[i].d_tail);
+        cudaFree(st.tails[i].d_rays);
+    }
     for (int i = 0; i < st.n_fy_tables; ++i) {
         cudaFree(st.fy_tables[i].d_fy);
         if (st.fy_tables[i].ready) cudaEventDestroy(st.fy_tables[i].ready);

@@ -243,6 +243,45 @@ def test_cooperative_tail_matches_reference(ref, labelled):
     v.close()
 
 
+def test_tail_launch_matches_reference(ref, labelled):
+    """Once most tiles of a VR frame have finished, the rays still marching
+    are handed (state and opacity caps) to a second launch that finishes
+    them with several lanes per ray.  Frames of fewer tiles than the hand-off
+    threshold hand over every ray still marching after 16 steps; larger ones
+    only the frame's tail.  Every image must equal MonkeyGL's and the frame
+    rendered without the hand-off, also when two streams render the same
+    volume at once (each stream has its own hand-off list)."""
+    import torch
+    w = labelled
+    lp = w.label_params.copy()
+    v = capi.Volume(w.phantom.volume)
+    v.set_mask(w.phantom.labels)
+    for l, lut in w.luts.items():
+        v.set_transfer_function(l, lut)
+    v.set_label_params(lp)
+    load_ref(ref, w)
+    frames = []
+    for ang, (W, H) in ((0.0, (1024, 768)), (65.0, (1024, 1024)), (130.0, (256, 256)), (200.0, (640, 360))):
+        p = capi.vr_params(W, H, 0, view_camera(ang), w.dims, w.spacing)
+        r = ref.render(W, H, 0, capi.vr_params_flat(p, lp))
+        m = v.render_vr(p)
+        assert_image_parity(m, r, f"tail {ang} {W}x{H}", exact=True)
+        p.flags = capi.VR_NO_TAIL
+        assert np.array_equal(v.render_vr(p), m), f"tail {ang}: differs from the frame without the hand-off"
+        p.flags = 0
+        frames.append((p, m))
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = [torch.empty(p.width * p.height * 3, dtype=torch.uint8, device="cuda") for p, _ in frames]
+    for rep in range(3):
+        for i, (p, _) in enumerate(frames):
+            v.render_vr_device(p, outs[i].data_ptr(), streams[i % 2].cuda_stream)
+        torch.cuda.synchronize()
+        for i, (p, m) in enumerate(frames):
+            got = outs[i].cpu().numpy().reshape(p.height, p.width, 3)
+            assert np.array_equal(got, m), f"two streams, frame {i} repeat {rep}"
+    v.close()
+
+
 def _plane(pl, mpr_type, sampling, spacing, half):
     return capi.plane_params(pl.width, pl.height, mpr_type, sampling, spacing, pl.dir_h, pl.dir_v,
                              pl.dir_n, pl.left_top, pl.pixel_spacing, False, half)
