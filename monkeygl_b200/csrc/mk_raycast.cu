@@ -52,9 +52,10 @@ namespace mk {
 // One 32x8 tile per block.  With `order`, block i renders tile order[i]
 // (index by * tiles_x + bx): the launch takes tiles centre first, where the
 // projected volume -- and the longest rays -- usually are, so they start in
-// the first wave instead of forming the tail of the launch.
+// the first wave instead of forming the tail of the launch.  Register
+// budgets: VR 64 (four blocks per SM), MIP and surface 40 (six).
 template <int MODE, int TRACK, bool COUNT>
-__global__ void __launch_bounds__(256) k_raycast(RayParams P, cudaTextureObject_t vol,
+__global__ void __launch_bounds__(256, MODE == kModeVR ? 4 : 6) k_raycast(RayParams P, cudaTextureObject_t vol,
                                                  cudaTextureObject_t mask, LabelTable LT,
                                                  BrickView BV, const int *__restrict__ order) {
     __shared__ LabelSmem S;
@@ -179,12 +180,19 @@ static void launch_raycast(int mode, int track, const RayParams &P, cudaTextureO
     }
 }
 
-// Tiles still unfinished when rays start to spill to the tail launch
-// (MONKEYGL_B200_TAIL_TILES overrides it; 0 spills from the first check).
+// Tiles still unfinished when rays start to spill to the tail launch:
+// two thirds of the SM count (measured on 1024^2 body frames on 148 SMs:
+// 16, 48, 96, 148, 296 tiles gave 2699, 2907, 2989, 2761, 2445 frames/s).
+// MONKEYGL_B200_TAIL_TILES overrides it (0: rays never spill).
 static int tail_tiles() {
     static const int k = [] {
         const char *e = getenv("MONKEYGL_B200_TAIL_TILES");
-        return e ? std::max(0, atoi(e)) : 296;
+        if (e) return std::max(0, atoi(e));
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        return std::max(1, 2 * sms / 3);
     }();
     return k;
 }
@@ -195,6 +203,7 @@ static int tail_tiles() {
 static int tail_params(VolumeState &v, RayParams &P, cudaStream_t s) {
     const int ntiles = ((P.W + 31) / 32) * ((P.H + 7) / 8);
     const int K = tail_tiles();
+    if (K == 0) return MK_OK;                      // no hand-off: P.tail stays null
     const int want = (int)std::min<long long>((long long)P.W * P.H, std::max(4LL * K * 256, 65536LL));
     int i = 0;
     while (i < v.n_tails && v.tails[i].stream != s) ++i;

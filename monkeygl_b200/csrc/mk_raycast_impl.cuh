@@ -511,8 +511,8 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             float4 clr = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             float alpha_j = 0.0f;
             int flags = 0, label = 0, nskip = 0;
+            float aj = Q.a;
             if (!Q.done) {
-                float aj = Q.a;
                 const int kj = Q.lat >= 0 ? min(Q.lat + j, P.accu_len - 1) : -1;
                 if (kj >= 0) aj = P.accu[kj];
                 else
@@ -561,11 +561,119 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             ws[lane].meta = flags | (label << 4) | (nskip << 12);
             __syncwarp();
 
-            // 2. MonkeyGL's schedule over the group's samples, in order
-            if (!Q.done) {
+            // 2. MonkeyGL's schedule over the group's samples, in order.
+            // In a round whose samples are all fetched (none outside the VOI,
+            // past the end or in a skipped brick) the step can change only
+            // where MonkeyGL's refinement test says so, and that test needs
+            // only sample j's alpha and the previous one: every lane decides
+            // whether the walk stops at its sample, the first stop ends the
+            // round, and only the compositing of the samples before it stays
+            // serial.  The ray's new position, step and previous alpha come
+            // from the stopping lane (the same float operations as the walk).
+            // Other rounds take the sample-by-sample walk.
+            const float alpha_up = __shfl_up_sync(FULL, alpha_j, 1);
+            const float pre_j = j == 0 ? Q.aPre : alpha_up;
+            const bool busy = (pre_j > alpha_j ? pre_j : alpha_j) > 0.001f;  // (alpha > aPre ? alpha : aPre) > 0.001
+            const bool pos_a = aj > 0.0f;
+            const bool refine_j = pos_a && busy && Q.step != L8;
+            const bool stop_j = !pos_a || Q.step == L4 || (Q.step == L1 ? busy : !busy);
+            const bool plain_j = (flags & (kCoopEnd | kCoopOutside | kCoopFetched)) == kCoopFetched;
+            const unsigned plain_m = __ballot_sync(FULL, plain_j);
+            const unsigned stop_m = __ballot_sync(FULL, stop_j);
+            const unsigned refine_m = __ballot_sync(FULL, refine_j);
+            const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
+            const bool simple = member && !Q.done && ((plain_m >> (g * G)) & gbits) == gbits;
+            const unsigned gstop = (stop_m >> (g * G)) & gbits;
+            const int s_at = gstop ? __ffs(gstop) - 1 : G;        // first stopping sample, G: none
+            const bool s_refine = s_at < G && ((refine_m >> (g * G + s_at)) & 1u);
+            {
+                // values of the stopping lane (or of the last lane when none stops)
+                const float ns = pos_a ? (Q.step == L8 ? L4 : L1) : Q.step;
+                float a_out, pre_out, step_out;
+                int lat_out;
+                if (s_at == G) {                    // all samples walked: a += step
+                    a_out = aj + Q.step;
+                    pre_out = alpha_j;
+                    step_out = Q.step;
+                    lat_out = Q.lat >= 0 ? Q.lat + G : Q.lat;
+                } else if (refine_j) {              // refine before compositing sample j
+                    a_out = Q.step == L1 ? aj - (L1 - L4) : aj - (L4 - L8);
+                    pre_out = pre_j;
+                    step_out = Q.step == L1 ? L4 : L8;
+                    lat_out = -1;
+                } else {                            // sample j walked, then the step coarsens
+                    a_out = aj + ns;
+                    pre_out = alpha_j;
+                    step_out = ns;
+                    lat_out = Q.lat >= 0 ? Q.lat + j + 1 : Q.lat;
+                }
+                const int src = g * G + (s_at < G ? s_at : G - 1);
+                const float a_new = __shfl_sync(FULL, a_out, src);
+                const float pre_new = __shfl_sync(FULL, pre_out, src);
+                const float step_new = __shfl_sync(FULL, step_out, src);
+                const int lat_new = __shfl_sync(FULL, lat_out, src);
+                if (simple) {
+                    const CoopSample *gs = ws + g * G;
+                    const int n_comp = s_at == G ? G : (s_refine ? s_at : s_at + 1);
+                    int c_lab = -1, c_slot = -2;
+                    float c_cap = 0.0f, c_acc = 0.0f;
+                    bool ended = false;
+                    float alpha_n = gs[0].alpha;
+                    int meta_n = gs[0].meta;
+                    float4 clr_n = gs[0].clr;
+                    for (int k = 0; k < n_comp; ++k) {
+                        const float alpha = alpha_n;
+                        const int lab = (meta_n >> 4) & 255;
+                        const float4 clr = clr_n;
+                        if (k + 1 < n_comp) {
+                            alpha_n = gs[k + 1].alpha;
+                            meta_n = gs[k + 1].meta;
+                            clr_n = gs[k + 1].clr;
+                        }
+                        if (alpha > 0.0005f) {
+                            if (lab != c_lab) {
+                                if (TRACK == kTrackShared && c_slot >= 0) s_acc[c_slot][owner_tid] = c_acc;
+                                c_lab = lab;
+                                c_slot = S.slot[lab];
+                                c_cap = S.alpha[lab];
+                                c_acc = (TRACK == kTrackShared && c_slot >= 0) ? s_acc[c_slot][owner_tid] : 0.0f;
+                            }
+                            const bool ok = c_slot != -2 && (c_slot == -1 || TRACK != kTrackShared || c_acc < c_cap);
+                            if (ok) {
+                                Q.sum = composite(Q.sum, Q.A, alpha, clr);
+                                if (TRACK == kTrackShared && c_slot >= 0) c_acc += (1.0f - Q.A) * alpha;
+                                Q.A += (1.0f - Q.A) * alpha;
+                                if (Q.A > 0.995f) {
+                                    ended = true;
+                                    break;
+                                }
+                            }
+                        }
+                    }
+                    if (TRACK == kTrackShared && c_slot >= 0) s_acc[c_slot][owner_tid] = c_acc;
+                    if (ended) {
+                        Q.done = true;
+                    } else {
+                        Q.a = a_new;
+                        Q.aPre = pre_new;
+                        Q.step = step_new;
+                        Q.lat = lat_new;
+                    }
+                }
+            }
+            if (!simple && !Q.done) {
+                // The walk is the serial part of a round, so nothing on its
+                // chain waits for shared memory: the next sample is read
+                // while this one is walked, and the opacity cap of the label
+                // last composited stays in registers (written back once).
+                const CoopSample *gs = ws + g * G;
+                int c_lab = -1, c_slot = -2;
+                float c_cap = 0.0f, c_acc = 0.0f;
                 int k = 0;
+                int meta = gs[0].meta;
+                float alpha_n = gs[0].alpha;
+                float4 clr_n = gs[0].clr;
                 while (k < G) {
-                    const int meta = ws[g * G + k].meta;
                     const int f = meta & 15;
                     if (f & kCoopEnd) {
                         Q.done = true;
@@ -574,7 +682,11 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     if (f & kCoopOutside) {
                         Q.a += Q.step;
                         if (Q.lat >= 0) ++Q.lat;
-                        ++k;
+                        if (++k < G) {
+                            meta = gs[k].meta;
+                            alpha_n = gs[k].alpha;
+                            clr_n = gs[k].clr;
+                        }
                         continue;
                     }
                     if ((f & kCoopEmpty) && P.skip && Q.step == L1 && Q.aPre <= 0.001f) {
@@ -582,10 +694,22 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                         Q.aPre = 0.0f;
                         advance_coarse(P, Q.a, Q.lat, Q.step, n);
                         k += n;
+                        if (k < G) {
+                            meta = gs[k].meta;
+                            alpha_n = gs[k].alpha;
+                            clr_n = gs[k].clr;
+                        }
                         continue;
                     }
                     if (!(f & kCoopFetched)) break;   // evaluate it in the next round
-                    const float alpha = ws[g * G + k].alpha;
+                    const float alpha = alpha_n;
+                    const float4 clr = clr_n;
+                    const int lab = (meta >> 4) & 255;
+                    if (k + 1 < G) {
+                        meta = gs[k + 1].meta;
+                        alpha_n = gs[k + 1].alpha;
+                        clr_n = gs[k + 1].clr;
+                    }
                     bool last = false;
                     if (Q.a > 0.0f) {
                         if ((alpha > Q.aPre ? alpha : Q.aPre) > 0.001f) {
@@ -611,10 +735,18 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     Q.a += Q.step;
                     if (Q.lat >= 0) ++Q.lat;
                     if (alpha > 0.0005f) {
-                        const int lab = (meta >> 4) & 255;
-                        if (vr_cap_ok<TRACK>(S, s_acc, nullptr, lab, owner_tid)) {
-                            Q.sum = composite(Q.sum, Q.A, alpha, ws[g * G + k].clr);
-                            vr_cap_add<TRACK>(S, s_acc, nullptr, lab, owner_tid, Q.A, alpha);
+                        if (lab != c_lab) {
+                            if (TRACK == kTrackShared && c_slot >= 0) s_acc[c_slot][owner_tid] = c_acc;
+                            c_lab = lab;
+                            c_slot = S.slot[lab];
+                            c_cap = S.alpha[lab];
+                            c_acc = (TRACK == kTrackShared && c_slot >= 0) ? s_acc[c_slot][owner_tid] : 0.0f;
+                        }
+                        // vr_cap_ok / vr_cap_add on the cached accumulator
+                        const bool ok = c_slot != -2 && (c_slot == -1 || TRACK != kTrackShared || c_acc < c_cap);
+                        if (ok) {
+                            Q.sum = composite(Q.sum, Q.A, alpha, clr);
+                            if (TRACK == kTrackShared && c_slot >= 0) c_acc += (1.0f - Q.A) * alpha;
                             Q.A += (1.0f - Q.A) * alpha;
                         }
                     }
@@ -625,6 +757,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     if (last) break;
                     ++k;
                 }
+                if (TRACK == kTrackShared && c_slot >= 0) s_acc[c_slot][owner_tid] = c_acc;
             }
             if (may_spill && (++round & 3) == 0 && tail_reached(P)) {
                 may_spill = false;
