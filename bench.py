@@ -198,11 +198,13 @@ def measured_peaks():
 
 
 def traffic_from_profile():
-    """DRAM bytes per launch of the VR kernel from the committed ncu summary."""
+    """DRAM bytes per frame of the VR launches (tile launch + tail launch)
+    from the committed ncu summary."""
     p = ROOT / "profiles" / "vr_body_1024_traffic.json"
     if p.exists():
         try:
-            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+            d = json.loads(p.read_text())
+            return d.get("dram_bytes_per_frame", d.get("dram_bytes_per_launch"))
         except (ValueError, OSError):
             return None
     return None
@@ -331,6 +333,11 @@ def run_mine(args, rank, local, world):
     achieved = b_alg / (mean_ms / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     gsps = mean_samples * (K / total_s) / 1e9
+    # a VR frame is two launches: the tiles, then the rays handed to the tail launch
+    tail = args.mode == "vr" and os.environ.get("MONKEYGL_B200_TAIL_TILES", "") != "0"
+    launches_per_frame = 2 if tail else 1
+    kernel_desc = (f"mk::k_raycast<{args.mode.upper()}> + mk::k_vr_tail (two launches per frame, timed together)"
+                   if tail else f"mk::k_raycast<{args.mode.upper()}> (one launch per frame)")
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "fps", "n_gpus": world, "steps": K,
@@ -348,10 +355,10 @@ def run_mine(args, rank, local, world):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic_from_profile(),
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
-                     "algorithmic_bytes_per_launch": int(b_alg),
-                     "kernel": f"mk::k_raycast<{args.mode.upper()}> (one launch per frame)"},
+                     "algorithmic_bytes_per_frame": int(b_alg),
+                     "kernel": kernel_desc},
         "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons", "samples")},
-        "gpu_launches": K,
+        "gpu_launches": K * launches_per_frame,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, views[0], size, rtype)

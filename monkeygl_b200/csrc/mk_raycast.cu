@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256, MODE == kModeVR ? 4 : 6) k_raycast(RayPar
 // allows (vr_coop_tail: groups of 32 / rays-per-warp lanes), writes their
 // pixels, and resets the frame's tail counters for the next frame.
 template <int TRACK>
-__global__ void __launch_bounds__(256) k_vr_tail(RayParams P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+__global__ void __launch_bounds__(256, 2) k_vr_tail(RayParams P, cudaTextureObject_t vol, cudaTextureObject_t mask,
                                                  LabelTable LT, BrickView BV) {
     __shared__ LabelSmem S;
     __shared__ float s_acc[TRACK == kTrackShared ? kMaxTrackedLabels : 1][256];
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256) k_vr_tail(RayParams P, cudaTextureObject_
         }
         const unsigned act = __ballot_sync(0xffffffffu, (unsigned)lane < cnt);
         __syncwarp();
-        vr_coop_tail<TRACK>(P, vol, mask, S, BV, s_acc, s_coop + (tid & ~31), act, R, dv, L, false);
+        vr_coop_tail<TRACK, true>(P, vol, mask, S, BV, s_acc, s_coop + (tid & ~31), act, R, dv, L, false);
         if ((unsigned)lane < cnt) {
             float4 sum = R.sum;
             if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;

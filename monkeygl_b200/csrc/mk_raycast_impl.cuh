@@ -462,7 +462,7 @@ __device__ __forceinline__ void vr_cap_add(const LabelSmem &S, float (*s_acc)[25
 // ray's final colour in R.sum.  Groups widen as rays finish: whenever the
 // unfinished rays fit into groups twice as large, their states move to new
 // groups, so a warp's last ray is marched by all 32 lanes.
-template <int TRACK>
+template <int TRACK, bool EARLY_TAPS = false>
 __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
                              const LabelSmem &S, const BrickView &BV, float (*s_acc)[256], CoopSample *ws,
                              unsigned act, VrRay &R, const StepVec &dv, float3 L, bool may_spill) {
@@ -514,9 +514,14 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             float aj = Q.a;
             if (!Q.done) {
                 const int kj = Q.lat >= 0 ? min(Q.lat + j, P.accu_len - 1) : -1;
-                if (kj >= 0) aj = P.accu[kj];
-                else
-                    for (int k = 0; k < j; ++k) aj += Q.step;
+                if (kj >= 0) {
+                    aj = P.accu[kj];
+                } else {
+                    // j sequential additions, as the walk makes them
+#pragma unroll
+                    for (int k = 0; k < 31; ++k)
+                        if (k < j) aj += Q.step;
+                }
                 if (!(aj < P.limit) || aj > Q.a_stop) {
                     flags = kCoopEnd;
                 } else {
@@ -541,6 +546,13 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                         if (!empty || (j == 0 && !(Q.aPre <= 0.001f))) {
                             label = mask ? min((int)tex3D<unsigned char>(mask, ix, iy, iz), MK_MAX_LABELS - 1) : 0;
                             float temp = 32768 * tex3D<float>(vol, pos.x, pos.y, pos.z);
+                            // (tail launch) a ray on a refined step is inside
+                            // something that composites: its shading taps are
+                            // fetched with the value, not after the LUT (one
+                            // texture round trip less, more registers)
+                            const bool early = EARLY_TAPS && Q.step != L1;
+                            GradTaps taps = {};
+                            if (early) taps = fetch_taps(vol, pos, P);
                             temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
                             if (temp > 1) temp = 1;
                             const cudaTextureObject_t tf = S.tf[label];
@@ -549,8 +561,10 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                             if (Q.step == L4) alpha = 1 - powf(1 - alpha, 0.25f);
                             else if (Q.step == L8) alpha = 1 - powf(1 - alpha, 0.125f);
                             alpha_j = alpha;
-                            if (alpha > 0.0005f)
-                                clr = shade_color(vol, pos, make_float4(col.x, col.y, col.z, alpha), L, P);
+                            if (alpha > 0.0005f) {
+                                if (!early) taps = fetch_taps(vol, pos, P);
+                                clr = shade_taps(taps, make_float4(col.x, col.y, col.z, alpha), L, P);
+                            }
                             flags |= kCoopFetched;
                         }
                     }
