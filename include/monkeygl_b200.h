@@ -187,6 +187,10 @@ int mk_volume_set_label_params(mk_volume vol, const float *alpha_ww_wl, int n_la
  * Replaces cu_render (core/kernel.cu:471-568).  `out` is host memory when
  * out_on_device == 0 (the call then returns with the image in `out`), else a
  * device pointer (the call returns after queuing the work on `stream`).
+ * A VR frame is two launches on `stream`: the tiles, then the rays still
+ * marching when all but a few tiles have finished (MK_VR_NO_TAIL: one
+ * launch).  The hand-off list is kept per volume and stream (four streams;
+ * created on a stream's first frame, grown for larger frames).
  */
 int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out,
                  int out_on_device, void *stream);
