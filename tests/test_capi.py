@@ -37,6 +37,18 @@ def test_binding_covers_header():
     assert set(declared_functions()) <= set(capi.exported_symbols())
 
 
+def test_header_constants_match_binding():
+    # every #define MK_* integer constant that the Python binding mirrors has the header's value
+    defines = dict((m.group(1), int(m.group(2), 0)) for m in
+                   re.finditer(r"^#define\s+MK_(\w+)\s+(0x[0-9a-fA-F]+|\d+)\b", HEADER.read_text(), re.M))
+    for name in ("VR_NO_SKIP", "VR_NO_COOP", "VR_NO_TAIL", "RENDER_VR", "RENDER_MIP", "RENDER_SURFACE"):
+        if name in defines and hasattr(capi, name):
+            assert getattr(capi, name) == defines[name], name
+    assert defines["VR_NO_TAIL"] == capi.VR_NO_TAIL
+    flags = [defines[n] for n in ("VR_NO_SKIP", "VR_NO_COOP", "VR_NO_TAIL")]
+    assert len(set(flags)) == 3 and all(f & (f - 1) == 0 for f in flags)   # distinct single bits
+
+
 def test_status_strings():
     L = capi.lib()
     assert L.mk_status_string(0) == b"ok"
