@@ -143,7 +143,10 @@ const char *mk_version(void);
 /*
  * Upload an int16 volume to `device` and build its brick occupancy map.
  * Replaces cu_copyVolumeData (core/CuDataManager.cu:28-73).  The host buffer
- * may be freed after the call returns.
+ * may be freed after the call returns.  A volume handle is used from one host
+ * thread at a time (its per-frame caches -- tile orders, ray parameter
+ * tables, hand-off lists -- are not locked); concurrent renders of one volume
+ * go through several streams from that thread, or through mk_server_*.
  */
 int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x, int dim_y,
                      int dim_z, int device);
