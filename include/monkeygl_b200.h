@@ -158,6 +158,17 @@ int mk_volume_device_bytes(mk_volume vol, size_t *bytes);
 int mk_volume_dims(mk_volume vol, int *dim_x, int *dim_y, int *dim_z);
 
 /*
+ * Introspection of the occupancy maps built at upload (no counterpart in
+ * MonkeyGL, which has none): nb = bricks along x, y, z (8^3 voxels each,
+ * numbered x fastest); minmax = 2 int16 per brick, the minimum and maximum
+ * voxel of the brick grown by one voxel on every side (clamped to the
+ * volume); labels = 3 words per brick, bit l set when label l (0..64)
+ * occurs among the brick's own voxels; present = 2 words, the labels
+ * occurring anywhere.  Any output pointer may be NULL; host memory.
+ */
+int mk_volume_brick_maps(mk_volume vol, int *nb, int16_t *minmax, uint32_t *labels, uint64_t *present);
+
+/*
  * Upload (labels != NULL) or remove (labels == NULL) the uint8 label volume,
  * same dims and layout as the voxels.  Replaces cu_copyMaskData
  * (core/CuDataManager.cu:75-120).
@@ -225,10 +236,15 @@ int mk_render_plane(mk_volume vol, const mk_plane_params *params, int16_t *out,
                     int out_on_device, void *stream);
 
 /*
- * Optional display epilogue for planes: window/level the int16 plane into
- * uint8 (0 below wl - ww/2, 255 above wl + ww/2, linear between).  MonkeyGL
- * applies this in its HTML client (cornerstone windowing set up in
- * examples/html/js/utils.js:40-60).
+ * Optional display epilogue for planes: the int16 plane of mk_render_plane
+ * windowed into uint8 exactly as MonkeyGL's HTML client displays it.  Its
+ * decodeMPR (examples/html/js/utils.js:62-118) hands ww 400 / wl 40 to
+ * cornerstone 0.12.2, which maps every value x to
+ * ((x - wl) / ww + 0.5) * 255 in double precision, clamped to [0, 255] and
+ * rounded to nearest with ties to even (a Uint8ClampedArray store,
+ * examples/html/js/libs/cornerstone@0.12.2.js:688-733).  The library builds
+ * that table for all 65536 int16 values on the host (64 KB of device memory
+ * per volume, allocated on the first call, rebuilt when ww or wl changes).
  */
 int mk_render_plane_u8(mk_volume vol, const mk_plane_params *params, float ww, float wl,
                        uint8_t *out, int out_on_device, void *stream);
@@ -306,7 +322,9 @@ int mk_dvr_backward(const mk_dvr_params *views, int nviews, const float *volume,
  *     that every GPU loading this library holds until the process exits;
  *     height > 4096 is rejected with MK_ERR_INVALID_ARGUMENT and a message.
  *   - The first call on a device looks up that array's device address; make
- *     that first call before any stream capture.
+ *     that first call before any stream capture.  The address is kept until
+ *     the process exits, so the call is not for use on a device after a
+ *     cudaDeviceReset in the same process.
  *   - The call is asynchronous on `stream` (NULL = the volume's stream).
  *     Every call shares the one array (each call overwrites the rows it
  *     uses; nothing needs to start at zero), so calls that overlap on the
@@ -376,6 +394,13 @@ typedef struct mk_server_config {
     int max_labels;              /* LUTs per request (labels 0..max_labels-1), 1..65 */
     int max_bricks;              /* largest volume, in 8^3 bricks; 0 = 512 x 512 x 2048 voxels */
     int tiles_per_step;          /* tiles of one batched launch; 0 = 8192 */
+    int evict_idle;              /* 0: a volume over the budget is refused (MK_ERR_BUDGET).
+                                    1: the server keeps a host copy of every volume; a volume that
+                                    does not fit, or a request for a volume evicted earlier, makes
+                                    room by evicting resident volumes that no admitted request
+                                    uses (least recently used first, those with no queued request
+                                    before those with one) and is uploaded on a loader thread
+                                    while requests for resident volumes keep running */
 } mk_server_config;
 
 enum { MK_REQUEST_VR = 0, MK_REQUEST_MIP = 1, MK_REQUEST_SURFACE = 2, MK_REQUEST_MPR = 3 };
@@ -399,6 +424,7 @@ typedef struct mk_request_times {
 
 typedef struct mk_server_stats {
     uint64_t submitted, completed, rejected, steps, tiles;
+    uint64_t evictions, loads;   /* volumes evicted / uploaded again (evict_idle) */
     size_t resident_bytes, budget_bytes;
     int volumes, slots_busy, pending;
 } mk_server_stats;
@@ -407,10 +433,13 @@ int mk_server_create(const mk_server_config *config, mk_server *out);
 /* Finish the work in flight, then release everything. */
 int mk_server_destroy(mk_server srv);
 /* Upload a volume (and its label volume, or NULL); MK_ERR_BUDGET when it does
- * not fit the budget beside the volumes already resident. */
+ * not fit the budget beside the volumes already resident (with evict_idle:
+ * only when it exceeds the budget on its own; otherwise idle volumes are
+ * evicted, or it is registered evicted and uploaded on its first request). */
 int mk_server_add_volume(mk_server srv, const int16_t *voxels, int dim_x, int dim_y, int dim_z,
                          const uint8_t *labels, int *volume_id);
-/* MK_ERR_NOT_READY while requests for the volume are queued or in flight. */
+/* MK_ERR_NOT_READY while requests for the volume are queued or in flight, or
+ * while it is being uploaded. */
 int mk_server_remove_volume(mk_server srv, int volume_id);
 /* Queue a request (its tables are copied); MK_ERR_QUEUE_FULL when max_pending
  * requests already wait for a slot. */

@@ -87,7 +87,7 @@ class ServerConfig(C.Structure):
     _fields_ = [
         ("device", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("max_slots", C.c_int),
         ("max_pending", C.c_int), ("max_pixels", C.c_int), ("lut_len", C.c_int), ("max_labels", C.c_int),
-        ("max_bricks", C.c_int), ("tiles_per_step", C.c_int),
+        ("max_bricks", C.c_int), ("tiles_per_step", C.c_int), ("evict_idle", C.c_int),
     ]
 
 
@@ -106,7 +106,8 @@ class RequestTimes(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [
         ("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64), ("steps", C.c_uint64),
-        ("tiles", C.c_uint64), ("resident_bytes", C.c_size_t), ("budget_bytes", C.c_size_t),
+        ("tiles", C.c_uint64), ("evictions", C.c_uint64), ("loads", C.c_uint64),
+        ("resident_bytes", C.c_size_t), ("budget_bytes", C.c_size_t),
         ("volumes", C.c_int), ("slots_busy", C.c_int), ("pending", C.c_int),
     ]
 
@@ -123,6 +124,8 @@ _SIGS = {
     "mk_volume_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "mk_volume_dims": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mk_volume_set_mask": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mk_volume_brick_maps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_uint64)]),
     "mk_volume_set_transfer_function": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "mk_volume_set_label_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "mk_render_vr": (C.c_int, [C.c_void_p, C.POINTER(VRParams), C.c_void_p, C.c_int, C.c_void_p]),
@@ -239,6 +242,19 @@ class Volume:
         if m.shape != self.dims[::-1]:
             raise ValueError("label volume shape differs from the voxels")
         _check(lib().mk_volume_set_mask(self.handle, _ptr(m)), "mk_volume_set_mask")
+
+    def brick_maps(self):
+        """(minmax (nbz, nby, nbx, 2) int16, labels (nbz, nby, nbx, 3) uint32,
+        present labels as a 65-entry bool array) of the occupancy maps."""
+        nb = (C.c_int * 3)()
+        _check(lib().mk_volume_brick_maps(self.handle, nb, None, None, None), "mk_volume_brick_maps")
+        nbx, nby, nbz = nb[0], nb[1], nb[2]
+        mm = np.empty((nbz, nby, nbx, 2), np.int16)
+        lab = np.empty((nbz, nby, nbx, 3), np.uint32)
+        pres = (C.c_uint64 * 2)()
+        _check(lib().mk_volume_brick_maps(self.handle, nb, _ptr(mm), _ptr(lab), pres), "mk_volume_brick_maps")
+        present = np.array([(pres[l >> 6] >> (l & 63)) & 1 for l in range(MAX_LABELS)], bool)
+        return mm, lab, present
 
     def set_transfer_function(self, label: int, lut: np.ndarray | None):
         if lut is None:

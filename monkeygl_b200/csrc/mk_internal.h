@@ -43,6 +43,23 @@ struct BrickView {
     int nbx, nby, nbz;
 };
 
+// The launches that read a cached device table, one event per reading
+// stream (recorded after the launch): before the table's memory is reused,
+// the host waits for those launches only.  A table read from more than
+// kTableStreams streams falls back to waiting for the device.
+constexpr int kTableStreams = 4;
+struct TableUses {
+    cudaStream_t stream[kTableStreams];
+    cudaEvent_t done[kTableStreams];
+    int n;
+    bool many;
+};
+// Record, on stream s, the end of the launches queued so far that read the table.
+int note_table_use(TableUses &u, cudaStream_t s);
+// Wait on the host until every recorded reader has finished, then forget them.
+int wait_table_uses(TableUses &u);
+void free_table_uses(TableUses &u);
+
 struct VolumeState {
     int device = 0;
     int dims[3] = {0, 0, 0};
@@ -85,9 +102,14 @@ struct VolumeState {
     struct TileOrder {
         int key[4];
         int *d_tiles;
+        int cap;                // ints the table holds
+        cudaEvent_t ready;      // recorded after the upload
+        TableUses uses;
+        uint64_t stamp;         // last use (least recently used is replaced)
     };
     TileOrder orders[16] = {};
     int n_orders = 0;
+    uint64_t order_clock = 0;
 
     // ray parameter (accu[k] - 0.866) * scale of every schedule entry, per
     // camera scale: samples on the table read it instead of evaluating it
@@ -95,14 +117,20 @@ struct VolumeState {
         float scale;
         float *d_fy;
         cudaEvent_t ready;      // recorded after the table is built
-        cudaEvent_t last_use;   // recorded after the last launch that read it
-        cudaStream_t user;      // stream of the launches that read it
-        bool shared;            // read from more than one stream
+        TableUses uses;
         uint64_t stamp;         // last use (least recently used is replaced)
     };
     FyTable fy_tables[8] = {};
     int n_fy_tables = 0;
     uint64_t fy_clock = 0;
+
+    // display window of mk_render_plane_u8: the uint8 value of every int16
+    // (index value + 32768) under the last (ww, wl) asked for
+    uint8_t *d_voi_lut = nullptr;
+    float voi_key[2] = {0.0f, 0.0f};
+    bool voi_valid = false;
+    cudaEvent_t voi_ready = nullptr;     // recorded after the table's upload
+    TableUses voi_uses = {};
 
     // VR frame tail: counters and spill list, one set per rendering stream
     // (the tile launch and the tail launch of a frame use them in stream

@@ -40,6 +40,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <utility>
 #include <vector>
 
@@ -130,7 +131,10 @@ __global__ void __launch_bounds__(256, 2) k_vr_tail(RayParams P, cudaTextureObje
         const unsigned act = __ballot_sync(0xffffffffu, (unsigned)lane < cnt);
         __syncwarp();
         vr_coop_tail<TRACK, true>(P, vol, mask, S, BV, s_acc, s_coop + (tid & ~31), act, R, dv, L, false);
-        if ((unsigned)lane < cnt) {
+        // the pixel index comes from the spill list: it is checked against
+        // the frame before the store, so a corrupt entry cannot write
+        // outside the image
+        if ((unsigned)lane < cnt && (unsigned)R.pix < (unsigned)P.W * (unsigned)P.H) {
             float4 sum = R.sum;
             if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;
             const uint32_t rgb = pack_rgb(sum);
@@ -238,13 +242,17 @@ static int tail_params(VolumeState &v, RayParams &P, cudaStream_t s) {
 template <int TRACK>
 static int launch_tail_track(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
                              const LabelTable &LT, const BrickView &BV, cudaStream_t s) {
-    static int grid = 0;
+    // one resident grid; computed once (threads that race here compute the
+    // same value)
+    static std::atomic<int> cached{0};
+    int grid = cached.load(std::memory_order_relaxed);
     if (grid == 0) {
         int dev = 0, sms = 0, per_sm = 0;
         MK_CUDA_TRY(cudaGetDevice(&dev));
         MK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         MK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_vr_tail<TRACK>, 256, 0));
         grid = std::max(1, sms * std::max(1, per_sm));
+        cached.store(grid, std::memory_order_relaxed);
     }
     k_vr_tail<TRACK><<<grid, 256, 0, s>>>(P, vol, mask, LT, BV);
     MK_CUDA_TRY(cudaGetLastError());
@@ -272,36 +280,85 @@ std::vector<int> centre_first_tiles(int W, int H, int xT, int yT) {
     return h;
 }
 
+int note_table_use(TableUses &u, cudaStream_t s) {
+    int i = 0;
+    while (i < u.n && u.stream[i] != s) ++i;
+    if (i == u.n) {
+        if (u.n == kTableStreams) {
+            u.many = true;                  // reuse will wait for the device
+            return MK_OK;
+        }
+        MK_CUDA_TRY(cudaEventCreateWithFlags(&u.done[i], cudaEventDisableTiming));
+        u.stream[i] = s;
+        ++u.n;
+    }
+    MK_CUDA_TRY(cudaEventRecord(u.done[i], s));
+    return MK_OK;
+}
+
+int wait_table_uses(TableUses &u) {
+    if (u.many) {
+        MK_CUDA_TRY(cudaDeviceSynchronize());
+    } else {
+        for (int i = 0; i < u.n; ++i) MK_CUDA_TRY(cudaEventSynchronize(u.done[i]));
+    }
+    free_table_uses(u);
+    return MK_OK;
+}
+
+void free_table_uses(TableUses &u) {
+    for (int i = 0; i < u.n; ++i) cudaEventDestroy(u.done[i]);
+    u.n = 0;
+    u.many = false;
+}
+
 // The centre-first tile order of a W x H image whose volume centre projects
 // to (W/2 + xT, H/2 + yT) (core/kernel.cu:161-162 with u = v = 0), cached on
-// the volume.  Tiles are sorted by the distance of their centre to that
-// point; a new table is uploaded on `s` and waited for once, so launches on
-// other streams can share it.
-static int tile_order(VolumeState &v, const RayParams &P, cudaStream_t s, const int **out) {
+// the volume (16 keys).  A new table is uploaded on `s` without a host wait;
+// launches on other streams that find it wait for its `ready` event.  The
+// caller records the launch that reads it with note_table_use(*idx); a
+// replaced table's memory is reused once those launches have finished.
+static int tile_order(VolumeState &v, const RayParams &P, cudaStream_t s, const int **out, int *idx) {
     const int key[4] = {P.W, P.H, (int)lrintf(P.xT), (int)lrintf(P.yT)};
     for (int i = 0; i < v.n_orders; ++i) {
-        const VolumeState::TileOrder &o = v.orders[i];
+        VolumeState::TileOrder &o = v.orders[i];
         if (o.key[0] == key[0] && o.key[1] == key[1] && o.key[2] == key[2] && o.key[3] == key[3]) {
+            MK_CUDA_TRY(cudaStreamWaitEvent(s, o.ready, 0));
+            o.stamp = ++v.order_clock;
             *out = o.d_tiles;
+            *idx = i;
             return MK_OK;
         }
     }
     const std::vector<int> h = centre_first_tiles(P.W, P.H, key[2], key[3]);
     const int n = (int)h.size();
-    if (v.n_orders == 16) {                      // drop the oldest
-        MK_CUDA_TRY(cudaStreamSynchronize(s));
-        cudaFree(v.orders[0].d_tiles);
-        for (int i = 1; i < 16; ++i) v.orders[i - 1] = v.orders[i];
-        v.n_orders = 15;
+    int i = v.n_orders;
+    if (i == 16) {                               // replace the least recently used
+        i = 0;
+        for (int j = 1; j < 16; ++j)
+            if (v.orders[j].stamp < v.orders[i].stamp) i = j;
+        int rc = wait_table_uses(v.orders[i].uses);
+        if (rc != MK_OK) return rc;
+    } else {
+        VolumeState::TileOrder o = {};
+        MK_CUDA_TRY(cudaEventCreateWithFlags(&o.ready, cudaEventDisableTiming));
+        v.orders[v.n_orders++] = o;
     }
-    int *dt = nullptr;
-    MK_CUDA_TRY(cudaMalloc(&dt, (size_t)n * sizeof(int)));
-    MK_CUDA_TRY(cudaMemcpyAsync(dt, h.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
-    MK_CUDA_TRY(cudaStreamSynchronize(s));
-    VolumeState::TileOrder &o = v.orders[v.n_orders++];
+    VolumeState::TileOrder &o = v.orders[i];
+    if (o.cap < n) {
+        cudaFree(o.d_tiles);
+        o.d_tiles = nullptr;
+        o.cap = 0;
+        MK_CUDA_TRY(cudaMalloc(&o.d_tiles, (size_t)n * sizeof(int)));
+        o.cap = n;
+    }
+    // pageable source: the call returns once `h` is staged
+    MK_CUDA_TRY(cudaMemcpyAsync(o.d_tiles, h.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s));
+    MK_CUDA_TRY(cudaEventRecord(o.ready, s));
     for (int k = 0; k < 4; ++k) o.key[k] = key[k];
-    o.d_tiles = dt;
-    *out = dt;
+    o.stamp = ++v.order_clock;
+    *out = o.d_tiles;
+    *idx = i;
     return MK_OK;
 }
 
@@ -321,19 +378,17 @@ int launch_fy_table(const VolumeState &v, float scale, float *out, cudaStream_t 
 // The fy table of volume v at `scale`, cached on the volume (8 scales).  A
 // new table is built on `s` without waiting: launches on `s` follow it in
 // stream order, and a launch on another stream that finds it in the cache
-// waits for its `ready` event.  The caller records `*used` on its stream after
-// the launch that reads the table; replacing the least recently used table (a
-// ninth scale) waits on the host for that event, or for the whole device when
-// the table was read from more than one stream.
-int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, cudaEvent_t *used) {
+// waits for its `ready` event.  The caller records the launch that reads it
+// with note_table_use(*idx); replacing the least recently used table (a
+// ninth scale) waits on the host for the launches recorded on it.
+int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, int *idx) {
     for (int i = 0; i < v.n_fy_tables; ++i) {
         VolumeState::FyTable &t = v.fy_tables[i];
         if (memcmp(&t.scale, &scale, sizeof(float)) == 0) {
             MK_CUDA_TRY(cudaStreamWaitEvent(s, t.ready, 0));
-            t.shared |= s != t.user;
             t.stamp = ++v.fy_clock;
             *out = t.d_fy;
-            *used = t.last_use;
+            *idx = i;
             return MK_OK;
         }
     }
@@ -342,17 +397,12 @@ int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, cud
         i = 0;
         for (int j = 1; j < 8; ++j)
             if (v.fy_tables[j].stamp < v.fy_tables[i].stamp) i = j;
-        if (v.fy_tables[i].shared) {
-            MK_CUDA_TRY(cudaDeviceSynchronize());
-        } else {
-            MK_CUDA_TRY(cudaEventSynchronize(v.fy_tables[i].last_use));
-        }
+        int rc = wait_table_uses(v.fy_tables[i].uses);
+        if (rc != MK_OK) return rc;
     } else {
         VolumeState::FyTable t = {};
         MK_CUDA_TRY(cudaMalloc(&t.d_fy, (size_t)v.accu_len * sizeof(float)));
-        if (cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&t.last_use, cudaEventDisableTiming) != cudaSuccess) {
-            if (t.ready) cudaEventDestroy(t.ready);
+        if (cudaEventCreateWithFlags(&t.ready, cudaEventDisableTiming) != cudaSuccess) {
             cudaFree(t.d_fy);
             set_last_error("fy table: event creation failed");
             return MK_ERR_CUDA;
@@ -364,11 +414,9 @@ int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, cud
     if (rc != MK_OK) return rc;
     MK_CUDA_TRY(cudaEventRecord(t.ready, s));
     t.scale = scale;
-    t.user = s;
-    t.shared = false;
     t.stamp = ++v.fy_clock;
     *out = t.d_fy;
-    *used = t.last_use;
+    *idx = i;
     return MK_OK;
 }
 
@@ -467,10 +515,10 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     rc = rebuild_brick_maps(&v, s);
     if (rc != MK_OK) return rc;
     const int *order = nullptr;
-    rc = tile_order(v, P, s, &order);
+    int order_idx = 0, fy_idx = 0;
+    rc = tile_order(v, P, s, &order, &order_idx);
     if (rc != MK_OK) return rc;
-    cudaEvent_t fy_used = nullptr;
-    rc = fy_table(v, P.scale, s, &P.fy_tab, &fy_used);
+    rc = fy_table(v, P.scale, s, &P.fy_tab, &fy_idx);
     if (rc != MK_OK) return rc;
     const int track = tracking_mode(v);
     const bool tail = params->render_type == MK_RENDER_VR && track != kTrackLocal &&
@@ -486,7 +534,9 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
         rc = launch_vr_tail(track, P, v.tex_linear, v.tex_mask, label_table(&v), brick_view(&v), s);
         if (rc != MK_OK) return rc;
     }
-    MK_CUDA_TRY(cudaEventRecord(fy_used, s));
+    rc = note_table_use(v.orders[order_idx].uses, s);
+    if (rc == MK_OK) rc = note_table_use(v.fy_tables[fy_idx].uses, s);
+    if (rc != MK_OK) return rc;
     return finish_output(&v, out, bytes, out_on_device, s);
 }
 

@@ -499,7 +499,10 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             T.sum.w = __shfl_sync(FULL, Q.sum.w, src);
             T.lat = __shfl_sync(FULL, Q.lat, src);
             T.pix = __shfl_sync(FULL, Q.pix, src);
-            owner = __shfl_sync(FULL, owner, src);
+            // masked to a lane: a shuffled value indexes the warp's own
+            // slices of s_acc and ws, so even a value from a lane that did
+            // not take part cannot address outside them
+            owner = __shfl_sync(FULL, owner, src) & 31;
             T.done = !member;
             Q = T;
         }
@@ -1207,8 +1210,8 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
 int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P);
 // Host: the ray parameter of every schedule entry at `scale` (cached on the
 // volume); rendering kernels read it for the samples on the table.
-// The caller records *used on s after its launch that reads the table.
-int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, cudaEvent_t *used);
+// The caller records its launch that reads table *idx with note_table_use.
+int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, int *idx);
 // Host: build that table into `out` (v.accu_len floats) on stream s.
 int launch_fy_table(const VolumeState &v, float scale, float *out, cudaStream_t s);
 int tracking_mode_for(const uint64_t present[2], const float (*params)[3]);

@@ -16,6 +16,7 @@
 // 64-byte row segment; CPR rows share their (point, direction) pair through
 // shared memory.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include <mutex>
@@ -88,8 +89,53 @@ int fill_plane_params(const VolumeState &v, const mk_plane_params *p, PlaneParam
     P.invertZ = p->invert_z ? 1 : 0;
     P.halfNum = p->half_num;
     P.mode = p->mpr_type;
-    P.ww = 1.0f;
-    P.wl = 0.0f;
+    P.voi_lut = nullptr;
+    return MK_OK;
+}
+
+// The display window MonkeyGL's HTML client applies to an int16 plane:
+// decodeMPR (examples/html/js/utils.js:62-118) hands window width 400 and
+// centre 40 to cornerstone 0.12.2, whose generateLut
+// (examples/html/js/libs/cornerstone@0.12.2.js:688-733) evaluates
+// ((x - wc) / ww + 0.5) * 255 in double for every stored value x and keeps it
+// in a Uint8ClampedArray: NaN and values <= 0 give 0, values >= 255 give 255,
+// the rest round to nearest with ties to even.
+uint8_t voi_window_u8(int x, double ww, double wc) {
+    const double v = (((double)x - wc) / ww + 0.5) * 255.0;
+    if (!(v > 0.0)) return 0;
+    if (v >= 255.0) return 255;
+    const double f = floor(v);
+    if (f + 0.5 < v) return (uint8_t)(f + 1.0);
+    if (v < f + 0.5) return (uint8_t)f;
+    return (uint8_t)((((long)f) & 1) ? f + 1.0 : f);
+}
+
+// The table of that window for every int16 value, on the device: rebuilt
+// when (ww, wl) changes, after the launches that read the old one.
+static int voi_table(VolumeState &v, float ww, float wl, cudaStream_t s, const uint8_t **out) {
+    if (!v.d_voi_lut) {
+        MK_CUDA_TRY(cudaEventCreateWithFlags(&v.voi_ready, cudaEventDisableTiming));
+        MK_CUDA_TRY(cudaMalloc(&v.d_voi_lut, 65536));
+        v.device_bytes += 65536;
+        v.voi_valid = false;
+    }
+    if (v.voi_valid && v.voi_key[0] == ww && v.voi_key[1] == wl) {
+        MK_CUDA_TRY(cudaStreamWaitEvent(s, v.voi_ready, 0));
+        *out = v.d_voi_lut;
+        return MK_OK;
+    }
+    int rc = wait_table_uses(v.voi_uses);
+    if (rc != MK_OK) return rc;
+    std::vector<uint8_t> h(65536);
+    for (int i = 0; i < 65536; ++i) h[i] = voi_window_u8(i - 32768, (double)ww, (double)wl);
+    v.voi_valid = false;
+    // pageable source: the call returns once `h` is staged
+    MK_CUDA_TRY(cudaMemcpyAsync(v.d_voi_lut, h.data(), 65536, cudaMemcpyHostToDevice, s));
+    MK_CUDA_TRY(cudaEventRecord(v.voi_ready, s));
+    v.voi_key[0] = ww;
+    v.voi_key[1] = wl;
+    v.voi_valid = true;
+    *out = v.d_voi_lut;
     return MK_OK;
 }
 
@@ -140,10 +186,10 @@ extern "C" int mk_render_plane_u8(mk_volume vol, const mk_plane_params *params, 
     PlaneParams P;
     int rc = fill_plane_params(v, params, P);
     if (rc != MK_OK) return rc;
-    P.ww = ww;
-    P.wl = wl;
     cudaSetDevice(v.device);
     cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
+    rc = voi_table(v, ww, wl, s, &P.voi_lut);
+    if (rc != MK_OK) return rc;
     const size_t bytes = (size_t)P.W * P.H;
     void *dst = out;
     if (!out_on_device) {
@@ -154,6 +200,8 @@ extern "C" int mk_render_plane_u8(mk_volume vol, const mk_plane_params *params, 
     const cudaTextureObject_t tex = params->sampling == MK_SAMPLE_NEAREST ? v.tex_point : v.tex_linear;
     launch_plane<true>(P, tex, dst, s);
     MK_CUDA_TRY(cudaGetLastError());
+    rc = note_table_use(v.voi_uses, s);
+    if (rc != MK_OK) return rc;
     return finish_output(&v, out, bytes, out_on_device, s);
 }
 
@@ -243,7 +291,11 @@ extern "C" int mk_render_cpr_noalloc(mk_volume vol, int width, int height, const
     cudaStream_t s = stream ? (cudaStream_t)stream : v.stream;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     // first call on this device: look up the array's device address (the
-    // host-side name of a __device__ variable is not a device pointer)
+    // host-side name of a __device__ variable is not a device pointer).  The
+    // address belongs to the device's current context and is kept for the
+    // life of the process; a device reset (cudaDeviceReset) ends that context
+    // together with every volume created in it, and this entry point is not
+    // to be called on that device after a reset.
     if (!g_noalloc_rows_dev[v.device]) {
         void *ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_cpr_rows);

@@ -21,7 +21,7 @@ struct PlaneParams {
     int invertZ;
     float halfNum;
     int mode;
-    float ww, wl;      // u8 epilogue
+    const uint8_t *voi_lut;   // u8 epilogue: display value of int16 v at [v + 32768]
 };
 
 template <int MODE>
@@ -67,10 +67,9 @@ __device__ __forceinline__ void plane_tile(const PlaneParams &P, cudaTextureObje
     if (x >= P.W || y >= P.H) return;
     const short r = reslice_pixel<MODE>(P, tex, x, y);
     if (U8) {
-        // linear window: 0 at wl - ww/2, 255 at wl + ww/2
-        float g = ((float)r - (P.wl - 0.5f * P.ww)) / P.ww * 255.0f;
-        g = fminf(fmaxf(g, 0.0f), 255.0f);
-        static_cast<uint8_t *>(out)[(size_t)y * P.W + x] = (uint8_t)(g + 0.5f);
+        // display window: one table read per pixel (the table is built on
+        // the host; 64 KB, resident in L1/L2)
+        static_cast<uint8_t *>(out)[(size_t)y * P.W + x] = __ldg(P.voi_lut + ((int)r + 32768));
     } else {
         static_cast<short *>(out)[(size_t)y * P.W + x] = r;
     }

@@ -147,9 +147,16 @@ struct Slot {
 };
 
 struct ServerVolume {
-    mk_volume vol = nullptr;
-    size_t bytes = 0;
+    mk_volume vol = nullptr;            // nullptr while evicted (or being uploaded)
+    size_t bytes = 0;                   // device bytes while resident, else the estimate
     int users = 0;                      // requests queued or in flight
+    int in_slots = 0;                   // requests admitted into slots: they pin the volume
+    bool loading = false;               // queued for, or in, an upload by the loader thread
+    uint64_t last_use = 0;              // admission clock of the latest request
+    int dims[3] = {0, 0, 0};
+    // host copies for reloads (evict_idle only)
+    std::shared_ptr<const std::vector<int16_t>> host_vox;
+    std::shared_ptr<const std::vector<uint8_t>> host_lab;
 };
 
 struct Req {
@@ -204,7 +211,11 @@ struct mk_server_s {
     std::deque<uint64_t> pending;
     std::vector<uint64_t> active;       // in slots, admission order
     std::deque<Step> inflight;
-    uint64_t next_ticket = 1, step_count = 0;
+    uint64_t next_ticket = 1, step_count = 0, use_clock = 0;
+    // evict_idle: volumes waiting for an upload, and the thread that does it
+    std::deque<int> load_queue;
+    std::condition_variable cv_load;
+    std::thread loader;
     mk_server_stats stats;
     bool stop = false;
     int fatal = MK_OK;
@@ -456,14 +467,20 @@ void worker_loop(mk_server_s *s) {
                 s->slots[q.slot].ticket = 0;
                 s->active.erase(std::find(s->active.begin(), s->active.end(), t));
                 auto it = s->volumes.find(q.r.volume);
-                if (it != s->volumes.end()) it->second.users--;
+                if (it != s->volumes.end()) {
+                    it->second.users--;
+                    it->second.in_slots--;
+                }
                 s->stats.completed++;
             }
             s->cv_done.notify_all();
+            if (!s->load_queue.empty()) s->cv_load.notify_one();   // volumes may be evictable now
             progressed = true;
         }
-        // 2. admit waiting requests into free slots
-        while (rc == MK_OK && !s->pending.empty()) {
+        // 2. admit waiting requests into free slots, in arrival order; a
+        //    request whose volume is not resident waits for the loader
+        //    thread (which it wakes) and does not hold up later requests
+        for (auto pit = s->pending.begin(); rc == MK_OK && pit != s->pending.end();) {
             int free_slot = -1;
             for (int i = 0; i < (int)s->slots.size(); ++i)
                 if (s->slots[i].ticket == 0) {
@@ -471,9 +488,21 @@ void worker_loop(mk_server_s *s) {
                     break;
                 }
             if (free_slot < 0) break;
-            const uint64_t t = s->pending.front();
-            s->pending.pop_front();
+            const uint64_t t = *pit;
+            ServerVolume &V = s->volumes[s->reqs[t].r.volume];
+            if (!V.vol || V.loading) {
+                if (!V.loading) {
+                    V.loading = true;
+                    s->load_queue.push_back(s->reqs[t].r.volume);
+                    s->cv_load.notify_one();
+                }
+                ++pit;
+                continue;
+            }
+            pit = s->pending.erase(pit);
             rc = admit(s, t, free_slot);
+            V.in_slots++;
+            V.last_use = ++s->use_clock;
             s->active.push_back(t);
             progressed = true;
         }
@@ -505,6 +534,119 @@ void worker_loop(mk_server_s *s) {
                 s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
             }
         }
+    }
+}
+
+// Resident volumes that may be evicted to make room for `need` more bytes:
+// those no admitted request uses, least recently used first, volumes with
+// no queued request before those with one.  Empty if they are not enough
+// (lock held).
+std::vector<int> eviction_victims(mk_server_s *s, int keep, size_t need) {
+    std::vector<std::pair<std::pair<int, uint64_t>, int>> cand;
+    for (auto &kv : s->volumes) {
+        const ServerVolume &V = kv.second;
+        if (kv.first == keep || !V.vol || V.loading || V.in_slots > 0) continue;
+        cand.push_back({{V.users > 0 ? 1 : 0, V.last_use}, kv.first});
+    }
+    std::sort(cand.begin(), cand.end());
+    std::vector<int> out;
+    size_t freed = 0;
+    for (auto &c : cand) {
+        if (s->resident + need <= s->budget + freed) break;
+        out.push_back(c.second);
+        freed += s->volumes[c.second].bytes;
+    }
+    if (s->resident + need > s->budget + freed) out.clear();
+    return out;
+}
+
+// Upload of one volume from its host copy (evict_idle); the caller reserved
+// `est` bytes of the budget.  Returns the handle or nullptr (status in rc).
+mk_volume upload_volume(const mk_server_s *s, const ServerVolume &V, int &rc) {
+    mk_volume v = nullptr;
+    rc = mk_volume_create(&v, V.host_vox->data(), V.dims[0], V.dims[1], V.dims[2], s->cfg.device);
+    if (rc == MK_OK && V.host_lab) rc = mk_volume_set_mask(v, V.host_lab->data());
+    if (rc == MK_OK) rc = mk_volume_synchronize(v, nullptr);
+    if (rc != MK_OK && v) {
+        mk_volume_destroy(v);
+        v = nullptr;
+    }
+    return v;
+}
+
+size_t volume_estimate(int dx, int dy, int dz, bool labels);
+
+// evict_idle: uploads evicted volumes that requests wait for, evicting idle
+// ones to make room.  Runs beside the worker, so steps of requests for
+// resident volumes continue during an upload.
+void loader_loop(mk_server_s *s) {
+    cudaSetDevice(s->cfg.device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        if (s->stop) break;
+        if (s->load_queue.empty()) {
+            s->cv_load.wait_for(lk, std::chrono::milliseconds(20));
+            continue;
+        }
+        const int id = s->load_queue.front();
+        auto it = s->volumes.find(id);
+        if (it == s->volumes.end() || it->second.vol) {
+            if (it != s->volumes.end()) it->second.loading = false;
+            s->load_queue.pop_front();
+            continue;
+        }
+        ServerVolume &V = it->second;
+        const size_t est = volume_estimate(V.dims[0], V.dims[1], V.dims[2], V.host_lab != nullptr);
+        std::vector<int> victims = eviction_victims(s, id, est);
+        if (s->resident + est > s->budget && victims.empty()) {
+            // every resident volume is in use: wait for requests to retire
+            s->cv_load.wait_for(lk, std::chrono::milliseconds(5));
+            continue;
+        }
+        s->load_queue.pop_front();
+        std::vector<mk_volume> dead;
+        for (int vid : victims) {
+            ServerVolume &E = s->volumes[vid];
+            dead.push_back(E.vol);
+            E.vol = nullptr;
+            s->resident -= E.bytes;
+            E.bytes = volume_estimate(E.dims[0], E.dims[1], E.dims[2], E.host_lab != nullptr);
+            s->stats.evictions++;
+        }
+        s->resident += est;                     // reserved while uploading
+        lk.unlock();
+        for (mk_volume d : dead) mk_volume_destroy(d);
+        int rc = MK_OK;
+        mk_volume v = upload_volume(s, V, rc);  // V stays in the map: only this thread erases loading volumes
+        size_t bytes = 0;
+        if (v) mk_volume_device_bytes(v, &bytes);
+        lk.lock();
+        s->resident -= est;
+        V.loading = false;
+        if (v) {
+            V.vol = v;
+            V.bytes = bytes;
+            s->resident += bytes;
+            s->stats.loads++;
+        } else {
+            // the requests waiting for this volume fail with the upload's status
+            const std::string msg = "mk_server: upload of an evicted volume failed";
+            for (auto pit = s->pending.begin(); pit != s->pending.end();) {
+                Req &q = s->reqs[*pit];
+                if (q.r.volume != id) {
+                    ++pit;
+                    continue;
+                }
+                q.done = true;
+                q.status = rc;
+                q.t_done = s->now_ms();
+                V.users--;
+                pit = s->pending.erase(pit);
+            }
+            set_last_error(msg);
+            s->cv_done.notify_all();
+        }
+        s->cv_work.notify_all();
     }
 }
 
@@ -668,6 +810,7 @@ extern "C" int mk_server_create(const mk_server_config *config, mk_server *out) 
     s->stats.budget_bytes = s->budget;
     s->t0 = Clock::now();
     s->worker = std::thread(worker_loop, s);
+    if (c.evict_idle) s->loader = std::thread(loader_loop, s);
     *out = s;
     return MK_OK;
 }
@@ -680,6 +823,8 @@ extern "C" int mk_server_destroy(mk_server s) {
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
+    s->cv_load.notify_all();
+    if (s->loader.joinable()) s->loader.join();
     cudaSetDevice(s->cfg.device);
     cudaStreamSynchronize(s->stream);
     cudaStreamSynchronize(s->step_stream[0]);
@@ -702,14 +847,49 @@ extern "C" int mk_server_add_volume(mk_server s, const int16_t *voxels, int dim_
         return MK_ERR_INVALID_ARGUMENT;
     }
     const size_t est = volume_estimate(dim_x, dim_y, dim_z, labels != nullptr);
+    const size_t nvox = (size_t)dim_x * dim_y * dim_z;
+    ServerVolume sv;
+    sv.dims[0] = dim_x;
+    sv.dims[1] = dim_y;
+    sv.dims[2] = dim_z;
+    if (s->cfg.evict_idle) {
+        if (est + s->slot_bytes > s->budget) {
+            set_last_error("mk_server_add_volume: the volume alone exceeds the HBM budget");
+            return MK_ERR_BUDGET;
+        }
+        sv.host_vox = std::make_shared<const std::vector<int16_t>>(voxels, voxels + nvox);
+        if (labels) sv.host_lab = std::make_shared<const std::vector<uint8_t>>(labels, labels + nvox);
+    }
+    std::vector<mk_volume> dead;
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->resident + est > s->budget) {
-            set_last_error("mk_server_add_volume: the volume does not fit the HBM budget");
-            return MK_ERR_BUDGET;
+            std::vector<int> victims;
+            if (s->cfg.evict_idle) victims = eviction_victims(s, -1, est);
+            if (victims.empty()) {
+                if (!s->cfg.evict_idle) {
+                    set_last_error("mk_server_add_volume: the volume does not fit the HBM budget");
+                    return MK_ERR_BUDGET;
+                }
+                // registered evicted: uploaded for its first request
+                const int id = s->next_volume++;
+                sv.bytes = est;
+                s->volumes[id] = sv;
+                *volume_id = id;
+                return MK_OK;
+            }
+            for (int vid : victims) {
+                ServerVolume &E = s->volumes[vid];
+                dead.push_back(E.vol);
+                E.vol = nullptr;
+                s->resident -= E.bytes;
+                E.bytes = volume_estimate(E.dims[0], E.dims[1], E.dims[2], E.host_lab != nullptr);
+                s->stats.evictions++;
+            }
         }
         s->resident += est;                      // reserved while uploading
     }
+    for (mk_volume d : dead) mk_volume_destroy(d);
     mk_volume v = nullptr;
     int rc = mk_volume_create(&v, voxels, dim_x, dim_y, dim_z, s->cfg.device);
     if (rc == MK_OK && labels) rc = mk_volume_set_mask(v, labels);
@@ -723,9 +903,9 @@ extern "C" int mk_server_add_volume(mk_server s, const int16_t *voxels, int dim_
         return rc;
     }
     const int id = s->next_volume++;
-    ServerVolume sv;
     sv.vol = v;
     sv.bytes = bytes;
+    sv.last_use = ++s->use_clock;
     s->volumes[id] = sv;
     s->resident += bytes;
     *volume_id = id;
@@ -742,15 +922,16 @@ extern "C" int mk_server_remove_volume(mk_server s, int volume_id) {
             set_last_error("mk_server_remove_volume: unknown volume");
             return MK_ERR_INVALID_ARGUMENT;
         }
-        if (it->second.users > 0) {
-            set_last_error("mk_server_remove_volume: requests for the volume are queued or in flight");
+        if (it->second.users > 0 || it->second.loading) {
+            set_last_error("mk_server_remove_volume: requests for the volume are queued or in flight, "
+                           "or it is being uploaded");
             return MK_ERR_NOT_READY;
         }
         v = it->second.vol;
-        s->resident -= it->second.bytes;
+        if (v) s->resident -= it->second.bytes;
         s->volumes.erase(it);
     }
-    return mk_volume_destroy(v);
+    return v ? mk_volume_destroy(v) : MK_OK;
 }
 
 extern "C" int mk_server_submit(mk_server s, const mk_request *req, uint64_t *ticket) {
@@ -768,7 +949,11 @@ extern "C" int mk_server_submit(mk_server s, const mk_request *req, uint64_t *ti
         set_last_error("mk_server_submit: unknown volume");
         return MK_ERR_INVALID_ARGUMENT;
     }
-    const VolumeState &vs = vit->second.vol->st;
+    // parameters are validated against the volume's dims (an evicted
+    // volume has no device state; a stand-in carries its dims)
+    VolumeState dims_only;
+    for (int k = 0; k < 3; ++k) dims_only.dims[k] = vit->second.dims[k];
+    const VolumeState &vs = vit->second.vol ? vit->second.vol->st : dims_only;
     Req q;
     q.r = *req;
     const int L = s->cfg.lut_len;

@@ -112,6 +112,187 @@ __global__ void __launch_bounds__(256) k_brick_labels(const unsigned char *__res
     if (lane < 3) out[3 * (size_t)b + lane] = lane == 0 ? m0 : (lane == 1 ? m1 : m2);
 }
 
+// The same two maps by rows of vectors, for volumes whose rows split into
+// whole bricks (dim_x a multiple of 8, at most 256 bricks across): thread t
+// of a block owns x-brick t of one brick row (blockIdx.x) for a run of
+// kZRun z-bricks (blockIdx.y), reads each voxel row of its brick as one
+// 16-byte vector (8 int16) and keeps packed min/max with the paired-int16
+// SIMD instructions.  The x halo of a row -- the last voxel of the brick to
+// the left, the first of the brick to the right -- comes from the
+// neighbouring lanes by shuffle (lanes 0 and 31 read it).  Slices are read
+// once per run: the slice below a brick and its first slice are both
+// carried in registers from the previous brick.  Every load of a warp is a
+// contiguous 512-byte row segment; the y halo rows are the neighbouring
+// brick rows' own rows, read again from L2.
+constexpr int kZRun = 4;
+
+struct Mm8 {
+    uint4 lo, hi;      // packed int16 min / max over x = x0..x0+7
+    int hlo, hhi;      // min / max of the x-halo voxels
+};
+
+__device__ __forceinline__ void mm8_init(Mm8 &m) {
+    m.lo = make_uint4(0x7fff7fffu, 0x7fff7fffu, 0x7fff7fffu, 0x7fff7fffu);
+    m.hi = make_uint4(0x80008000u, 0x80008000u, 0x80008000u, 0x80008000u);
+    m.hlo = 32767;
+    m.hhi = -32768;
+}
+
+__device__ __forceinline__ void mm8_merge(Mm8 &a, const Mm8 &b) {
+    a.lo.x = __vmins2(a.lo.x, b.lo.x);
+    a.lo.y = __vmins2(a.lo.y, b.lo.y);
+    a.lo.z = __vmins2(a.lo.z, b.lo.z);
+    a.lo.w = __vmins2(a.lo.w, b.lo.w);
+    a.hi.x = __vmaxs2(a.hi.x, b.hi.x);
+    a.hi.y = __vmaxs2(a.hi.y, b.hi.y);
+    a.hi.z = __vmaxs2(a.hi.z, b.hi.z);
+    a.hi.w = __vmaxs2(a.hi.w, b.hi.w);
+    a.hlo = min(a.hlo, b.hlo);
+    a.hhi = max(a.hhi, b.hhi);
+}
+
+// Min/max of slice z over the brick's x range grown by one voxel and the
+// ten rows yrow[0..9] (the brick's rows grown by one, clamped).  Called by
+// every lane of the warp (the shuffles need all 32).
+__device__ __forceinline__ Mm8 mm8_slice(const short *__restrict__ vox, size_t zoff, int dx, const int *yrow,
+                                         int x0, int lane, bool left, bool right) {
+    Mm8 m;
+    mm8_init(m);
+    uint4 v[10];
+#pragma unroll
+    for (int r = 0; r < 10; ++r)
+        v[r] = __ldg(reinterpret_cast<const uint4 *>(vox + zoff + (size_t)yrow[r] * dx + x0));
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        m.lo.x = __vmins2(m.lo.x, v[r].x);
+        m.lo.y = __vmins2(m.lo.y, v[r].y);
+        m.lo.z = __vmins2(m.lo.z, v[r].z);
+        m.lo.w = __vmins2(m.lo.w, v[r].w);
+        m.hi.x = __vmaxs2(m.hi.x, v[r].x);
+        m.hi.y = __vmaxs2(m.hi.y, v[r].y);
+        m.hi.z = __vmaxs2(m.hi.z, v[r].z);
+        m.hi.w = __vmaxs2(m.hi.w, v[r].w);
+        int l = (short)(__shfl_up_sync(0xffffffffu, v[r].w, 1) >> 16);     // voxel x0 - 1
+        int h = (short)(__shfl_down_sync(0xffffffffu, v[r].x, 1) & 0xffffu); // voxel x0 + 8
+        if (lane == 0 && left) l = __ldg(vox + zoff + (size_t)yrow[r] * dx + x0 - 1);
+        if (lane == 31 && right) h = __ldg(vox + zoff + (size_t)yrow[r] * dx + x0 + 8);
+        if (!left) l = (short)(v[r].x & 0xffffu);
+        if (!right) h = (short)(v[r].w >> 16);
+        m.hlo = min(m.hlo, min(l, h));
+        m.hhi = max(m.hhi, max(l, h));
+    }
+    return m;
+}
+
+__device__ __forceinline__ short2 mm8_result(const Mm8 &m) {
+    uint32_t lo = __vmins2(__vmins2(m.lo.x, m.lo.y), __vmins2(m.lo.z, m.lo.w));
+    uint32_t hi = __vmaxs2(__vmaxs2(m.hi.x, m.hi.y), __vmaxs2(m.hi.z, m.hi.w));
+    const int l = min(min((int)(short)(lo & 0xffffu), (int)(short)(lo >> 16)), m.hlo);
+    const int h = max(max((int)(short)(hi & 0xffffu), (int)(short)(hi >> 16)), m.hhi);
+    return make_short2((short)l, (short)h);
+}
+
+__global__ void __launch_bounds__(256) k_brick_minmax_rows(const short *__restrict__ vox, int dx, int dy, int dz,
+                                                            int nbx, int nby, int nbz, short2 *out) {
+    const int lane = threadIdx.x & 31;
+    const int bx = min((int)threadIdx.x, nbx - 1);   // lanes past the last brick repeat it and store nothing
+    const bool owner = (int)threadIdx.x < nbx;
+    const int by = blockIdx.x;
+    const int bz0 = blockIdx.y * kZRun, bz1 = min(bz0 + kZRun, nbz);
+    const int x0 = bx * kBrick;
+    const bool left = bx > 0, right = bx + 1 < nbx;
+    int yrow[10];
+#pragma unroll
+    for (int r = 0; r < 10; ++r) yrow[r] = min(max(by * kBrick - 1 + r, 0), dy - 1);
+    const size_t plane = (size_t)dx * dy;
+    const int za = max(bz0 * kBrick - 1, 0), zb = min(bz1 * kBrick, dz - 1);
+    Mm8 acc, prev;
+    mm8_init(acc);
+    mm8_init(prev);
+    int cur = bz0;
+    for (int z = za; z <= zb; ++z) {
+        const Mm8 S = mm8_slice(vox, (size_t)z * plane, dx, yrow, x0, lane, left, right);
+        mm8_merge(acc, S);
+        if ((z >> kBrickShift) > cur) {       // z = 8 (cur + 1): the slice above brick cur
+            if (owner) out[((size_t)cur * nby + by) * nbx + bx] = mm8_result(acc);
+            if (++cur >= bz1) break;
+            acc = prev;                       // the slice below brick cur, then its first slice
+            mm8_merge(acc, S);
+        }
+        prev = S;
+    }
+    if (cur < bz1 && owner) out[((size_t)cur * nby + by) * nbx + bx] = mm8_result(acc);
+}
+
+// Label sets by rows: thread t owns x-brick t of one brick row for kZRun
+// z-bricks, reads each 8-voxel row of its brick as one 8-byte word and sets
+// one bit per distinct label (a row of one label, the common case, sets one
+// bit).  The labels present anywhere in the volume are OR-ed into
+// `present` (3 words) once per warp.
+__device__ __forceinline__ void label_bits_word(uint32_t w, uint32_t &m0, uint32_t &m1, uint32_t &m2) {
+    if (w == (w & 0xffu) * 0x01010101u) {
+        int l = min((int)(w & 0xffu), 64);    // labels above MAXOBJECTCOUNT never occur via the API
+        if (l < 32) m0 |= 1u << l;
+        else if (l < 64) m1 |= 1u << (l - 32);
+        else m2 |= 1u;
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int l = min((int)((w >> (8 * k)) & 0xffu), 64);
+        if (l < 32) m0 |= 1u << l;
+        else if (l < 64) m1 |= 1u << (l - 32);
+        else m2 |= 1u;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_brick_labels_rows(const unsigned char *__restrict__ lab, int dx, int dy,
+                                                            int dz, int nbx, int nby, int nbz, uint32_t *out,
+                                                            uint32_t *present) {
+    const int bx = threadIdx.x;
+    uint32_t p0 = 0, p1 = 0, p2 = 0;
+    if (bx < nbx) {
+        const int by = blockIdx.x;
+        const int bz0 = blockIdx.y * kZRun, bz1 = min(bz0 + kZRun, nbz);
+        const int x0 = bx * kBrick;
+        const int y0 = by * kBrick, ny = min(kBrick, dy - y0);
+        const size_t plane = (size_t)dx * dy;
+        for (int bz = bz0; bz < bz1; ++bz) {
+            const int z0 = bz * kBrick, nz = min(kBrick, dz - z0);
+            uint32_t m0 = 0, m1 = 0, m2 = 0;
+            for (int z = z0; z < z0 + nz; ++z) {
+                const unsigned char *base = lab + (size_t)z * plane + (size_t)y0 * dx + x0;
+                uint2 w[kBrick];
+#pragma unroll
+                for (int r = 0; r < kBrick; ++r)
+                    w[r] = r < ny ? __ldg(reinterpret_cast<const uint2 *>(base + (size_t)r * dx)) : w[0];
+#pragma unroll
+                for (int r = 0; r < kBrick; ++r) {
+                    if (r < ny) {
+                        label_bits_word(w[r].x, m0, m1, m2);
+                        label_bits_word(w[r].y, m0, m1, m2);
+                    }
+                }
+            }
+            uint32_t *o = out + 3 * (((size_t)bz * nby + by) * nbx + bx);
+            o[0] = m0;
+            o[1] = m1;
+            o[2] = m2;
+            p0 |= m0;
+            p1 |= m1;
+            p2 |= m2;
+        }
+    }
+    p0 = __reduce_or_sync(0xffffffffu, p0);
+    p1 = __reduce_or_sync(0xffffffffu, p1);
+    p2 = __reduce_or_sync(0xffffffffu, p2);
+    if ((threadIdx.x & 31) == 0 && (p0 | p1 | p2)) {
+        atomicOr(&present[0], p0);
+        atomicOr(&present[1], p1);
+        atomicOr(&present[2], p2);
+    }
+}
+
 __global__ void k_fill_labels_zero(uint32_t *out, int nbricks) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b < nbricks) {
@@ -186,6 +367,10 @@ __global__ void __launch_bounds__(256) k_brick_visibility(const short2 *__restri
     const uint32_t word = __ballot_sync(0xffffffffu, vis);
     if ((threadIdx.x & 31) == 0 && b < nbricks + 31) vis_bits[b >> 5] = word;
 }
+
+// The row kernels apply when every row splits into whole bricks and a block
+// of one thread per x-brick stays within 256 threads.
+bool brick_rows_fit(int dim_x, int nbx) { return dim_x % kBrick == 0 && nbx <= 256; }
 
 int upload_linear(const void *host, size_t bytes, void **dptr, cudaStream_t s) {
     MK_CUDA_TRY(cudaMalloc(dptr, bytes));
@@ -436,8 +621,14 @@ extern "C" int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x
         st.device_bytes += nbricks * (sizeof(short2) + 3 * sizeof(uint32_t) + sizeof(float)) +
                            nwords * sizeof(uint32_t) + sizeof(unsigned long long);
         cudaMemsetAsync(st.d_visible, 0, nwords * sizeof(uint32_t), st.stream);
-        k_brick_minmax<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
-            (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], (int)nbricks, st.d_minmax);
+        if (brick_rows_fit(dim_x, st.nb[0])) {
+            const dim3 grid(st.nb[1], (st.nb[2] + kZRun - 1) / kZRun);
+            k_brick_minmax_rows<<<grid, (st.nb[0] + 31) & ~31, 0, st.stream>>>(
+                (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], st.nb[2], st.d_minmax);
+        } else {
+            k_brick_minmax<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
+                (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], (int)nbricks, st.d_minmax);
+        }
         k_fill_labels_zero<<<(unsigned)((nbricks + 255) / 256), 256, 0, st.stream>>>(
             st.d_labels, (int)nbricks);
         e = cudaGetLastError();
@@ -502,7 +693,11 @@ extern "C" int mk_volume_destroy(mk_volume v) {
     cudaFree(st.d_accu);
     cudaFree(st.d_out);
     cudaFree(st.d_counter);
-    for (int i = 0; i < st.n_orders; ++i) cudaFree(st.orders[i].d_tiles);
+    for (int i = 0; i < st.n_orders; ++i) {
+        cudaFree(st.orders[i].d_tiles);
+        if (st.orders[i].ready) cudaEventDestroy(st.orders[i].ready);
+        free_table_uses(st.orders[i].uses);
+    }
     for (int i = 0; i < st.n_tails; ++i) {
         cudaFree(st.tails[i].d_tail);
         cudaFree(st.tails[i].d_rays);
@@ -510,8 +705,11 @@ extern "C" int mk_volume_destroy(mk_volume v) {
     for (int i = 0; i < st.n_fy_tables; ++i) {
         cudaFree(st.fy_tables[i].d_fy);
         if (st.fy_tables[i].ready) cudaEventDestroy(st.fy_tables[i].ready);
-        if (st.fy_tables[i].last_use) cudaEventDestroy(st.fy_tables[i].last_use);
+        free_table_uses(st.fy_tables[i].uses);
     }
+    cudaFree(st.d_voi_lut);
+    if (st.voi_ready) cudaEventDestroy(st.voi_ready);
+    free_table_uses(st.voi_uses);
     if (st.h_pinned) cudaFreeHost(st.h_pinned);
     if (st.stream) cudaStreamDestroy(st.stream);
     cudaGetLastError();
@@ -522,6 +720,34 @@ extern "C" int mk_volume_destroy(mk_volume v) {
 extern "C" int mk_volume_device_bytes(mk_volume v, size_t *bytes) {
     if (!v || !bytes) return MK_ERR_INVALID_ARGUMENT;
     *bytes = v->st.device_bytes;
+    return MK_OK;
+}
+
+extern "C" int mk_volume_brick_maps(mk_volume v, int *nb, int16_t *minmax, uint32_t *labels,
+                                    uint64_t *present) {
+    if (!v) {
+        set_last_error("mk_volume_brick_maps: null volume");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &st = v->st;
+    if (nb) {
+        nb[0] = st.nb[0];
+        nb[1] = st.nb[1];
+        nb[2] = st.nb[2];
+    }
+    DeviceGuard guard(st.device);
+    const size_t nbricks = brick_count(&st);
+    if (minmax)
+        MK_CUDA_TRY(cudaMemcpyAsync(minmax, st.d_minmax, nbricks * sizeof(short2), cudaMemcpyDeviceToHost,
+                                    st.stream));
+    if (labels)
+        MK_CUDA_TRY(cudaMemcpyAsync(labels, st.d_labels, nbricks * 3 * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st.stream));
+    MK_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    if (present) {
+        present[0] = st.present_labels[0];
+        present[1] = st.present_labels[1];
+    }
     return MK_OK;
 }
 
@@ -580,26 +806,51 @@ extern "C" int mk_volume_set_mask(mk_volume v, const uint8_t *labels) {
             rc = MK_ERR_CUDA;
         }
     }
+    // labels present anywhere (used to size per-ray state): OR-ed on the
+    // device by the row kernel, else scanned on the host
+    const bool rows = brick_rows_fit(dx, st.nb[0]);
+    uint32_t h_present[3] = {0, 0, 0};
+    uint32_t *d_present = nullptr;
+    if (rc == MK_OK && rows && cudaMalloc(&d_present, 3 * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        set_last_error("mk_volume_set_mask: allocation failed");
+        rc = MK_ERR_OUT_OF_MEMORY;
+    }
     if (rc == MK_OK) {
-        k_brick_labels<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
-            (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], (int)nbricks, st.d_labels);
-        e = cudaGetLastError();
+        if (rows) {
+            e = cudaMemsetAsync(d_present, 0, 3 * sizeof(uint32_t), st.stream);
+            const dim3 grid(st.nb[1], (st.nb[2] + kZRun - 1) / kZRun);
+            if (e == cudaSuccess)
+                k_brick_labels_rows<<<grid, (st.nb[0] + 31) & ~31, 0, st.stream>>>(
+                    (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], st.nb[2], st.d_labels, d_present);
+        } else {
+            k_brick_labels<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
+                (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], (int)nbricks, st.d_labels);
+        }
+        if (e == cudaSuccess) e = cudaGetLastError();
+        if (e == cudaSuccess && rows)
+            e = cudaMemcpyAsync(h_present, d_present, sizeof(h_present), cudaMemcpyDeviceToHost, st.stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st.stream);
         if (e != cudaSuccess) {
             set_last_error(std::string("mk_volume_set_mask: ") + cudaGetErrorString(e));
             rc = MK_ERR_CUDA;
         }
     }
+    cudaFree(d_present);
     cudaFree(d_lin);
     if (rc != MK_OK) {
         free_mask(st);
         return rc;
     }
-    // labels present anywhere (host-side scan; used to size per-ray state)
     uint64_t pres[2] = {0, 0};
-    for (size_t i = 0; i < nvox; ++i) {
-        const int l = labels[i] > 64 ? 64 : labels[i];
-        pres[l >> 6] |= 1ull << (l & 63);
+    if (rows) {
+        pres[0] = (uint64_t)h_present[0] | ((uint64_t)h_present[1] << 32);
+        pres[1] = h_present[2] & 1u;
+    } else {
+        for (size_t i = 0; i < nvox; ++i) {
+            const int l = labels[i] > 64 ? 64 : labels[i];
+            pres[l >> 6] |= 1ull << (l & 63);
+        }
     }
     st.present_labels[0] = pres[0];
     st.present_labels[1] = pres[1];

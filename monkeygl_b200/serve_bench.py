@@ -118,24 +118,70 @@ def run_plain(vols, trace, pool, open_loop: bool):
     return lat, wall
 
 
-def main(args):
+def run_monkeygl(ref, trace, pool, open_loop: bool):
+    """The trace through MonkeyGL's own launchers (its core/kernel.cu and
+    core/CuDataManager.cu, oracle/_ref), one request per launch as its
+    HelloMonkey serves one: the request's LUTs through cu_setTransferFunc
+    (an array allocated per table), then cu_render (output allocated, kernel,
+    synchronous copy, free) or cu_renderPlane_*.  The volumes stay resident
+    in the harness's slots, which MonkeyGL's one-volume singleton cannot do,
+    so no upload is counted."""
+    from . import capi
+    b = pool.take()
+    lat = []
+    lp65 = np.zeros((capi.MAX_LABELS, 3), np.float32)
+    t0 = time.perf_counter()
+    for r in trace:
+        if open_loop:
+            dt = t0 + r.arrival_s - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+        ref.select(r.volume)
+        if r.kind == capi.REQUEST_MPR:
+            ref.plane(r.size, r.size, capi.plane_params_flat(r.plane), r.plane.mpr_type, r.plane.sampling)
+        else:
+            ref.clear_tfs()
+            n = r.luts.shape[0]
+            for l in range(n):
+                ref.set_lut(l, r.luts[l])
+            lp65[:] = (0.0, 1.0, 0.0)
+            lp65[:n] = r.label_params
+            out = pool.view(b, (r.size, r.size, 3), np.uint8)
+            ref.render_into(out, r.size, r.size, r.kind, np.ascontiguousarray(capi.vr_params_flat(r.vr, lp65)))
+        lat.append((time.perf_counter() - (t0 + (r.arrival_s if open_loop else 0.0))) * 1e3)
+    wall = time.perf_counter() - t0
+    pool.give(b)
+    return lat, wall
+
+
+def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True, log=None):
+    """The serving figures as a dict: the trace through the server, through
+    this library's one-launch-per-request path and (with `ref`, MonkeyGL's
+    kernels) through MonkeyGL's one-launch-per-request path; then an
+    eviction run (server with evict_idle under a budget below the four
+    volumes) when `evict`.  `phantoms` may pass the four serving phantoms
+    (workloads.SERVING_VOLUMES) already built."""
     import torch
     from . import capi
     from . import server as S
     from .phantom import make_phantom
     from .workloads import SERVING_VOLUMES, serving_trace
 
-    n = getattr(args, "serve_requests", 10000) or 10000
-    rate = getattr(args, "serve_rate", 200.0) or 200.0
-    nsat = min(n, getattr(args, "saturation", 2000) or 2000)
+    nsat = min(n, nsat)
     torch.cuda.init()
-    phantoms = [make_phantom(d, s, seed, with_labels=lab) for d, s, seed, lab in SERVING_VOLUMES]
+    if phantoms is None:
+        phantoms = [make_phantom(d, s, seed, with_labels=lab) for d, s, seed, lab in SERVING_VOLUMES]
     specs = [(p.dims, p.spacing, p.labels is not None) for p in phantoms]
     trace = serving_trace(specs, n, rate, seed=2024)
     pool = _Pool(64, 1024 * 1024 * 4)
 
     srv = S.Server(max_slots=32, max_pending=max(n, 1), max_pixels=1024 * 1024, max_labels=8)
-    vids = [srv.add_volume(p.volume, p.labels) for p in phantoms]
+    slot_bytes = srv.stats()["resident_bytes"]
+    vids, vol_bytes = [], []
+    for p in phantoms:
+        before = srv.stats()["resident_bytes"]
+        vids.append(srv.add_volume(p.volume, p.labels))
+        vol_bytes.append(srv.stats()["resident_bytes"] - before)
     plain_vols = []
     for p in phantoms:
         v = capi.Volume(p.volume)
@@ -190,5 +236,39 @@ def main(args):
         "p99_target_ms": 20.0,
     }
     line["saturation_latency"] = {"server": _pcts(sat_s_lat), "plain": _pcts(sat_p_lat)}
+    if ref is not None:
+        for i, p in enumerate(phantoms):
+            ref.select(i)
+            ref.set_volume(p.volume)
+            ref.set_mask(p.labels)
+        lat_m, wall_m = run_monkeygl(ref, trace, pool, open_loop=True)
+        sat_m_lat, sat_m = run_monkeygl(ref, trace[:nsat], pool, open_loop=False)
+        ref.select(0)
+        line["monkeygl_plain"] = {**_pcts(lat_m), "renders_per_s": round(n / wall_m, 1),
+                                  "saturation_renders_per_s": round(nsat / sat_m, 1)}
+        line["saturation_ratio_vs_monkeygl"] = round((nsat / sat_s) / (nsat / sat_m), 2)
+        line["saturation_latency"]["monkeygl_plain"] = _pcts(sat_m_lat)
+    if evict:
+        # the budget holds the slots and 70% of the four volumes: requests for
+        # an evicted volume wait for its upload while the others keep running
+        budget = int(slot_bytes + 0.7 * sum(vol_bytes))
+        ne = min(n, 2000)
+        with S.Server(max_slots=32, max_pending=max(ne, 1), max_pixels=1024 * 1024, max_labels=8,
+                      hbm_budget_bytes=budget, evict_idle=True) as es:
+            evids = [es.add_volume(p.volume, p.labels) for p in phantoms]
+            lat_e, wall_e = run_server(es, evids, trace[:ne], pool, open_loop=True)
+            est = es.stats()
+        line["eviction"] = {**_pcts(lat_e), "requests": ne, "renders_per_s": round(ne / wall_e, 1),
+                            "budget_mb": round(budget / 2 ** 20, 1),
+                            "volumes_mb": round(sum(vol_bytes) / 2 ** 20, 1),
+                            "evictions": est["evictions"], "loads": est["loads"]}
+    return line
+
+
+def main(args, ref=None):
+    n = getattr(args, "serve_requests", 10000) or 10000
+    rate = getattr(args, "serve_rate", 200.0) or 200.0
+    nsat = getattr(args, "saturation", 2000) or 2000
+    line = measure(n, rate, nsat, ref=ref)
     print(json.dumps(line), flush=True)
     return line

@@ -34,11 +34,11 @@ def _pinned_empty(shape, dtype):
 class Server:
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_slots: int = 32, max_pending: int = 4096,
                  max_pixels: int = 1024 * 1024, lut_len: int = 256, max_labels: int = 8, max_bricks: int = 0,
-                 tiles_per_step: int = 0):
+                 tiles_per_step: int = 0, evict_idle: bool = False):
         cfg = capi.ServerConfig()
         cfg.device, cfg.hbm_budget_bytes, cfg.max_slots, cfg.max_pending = device, hbm_budget_bytes, max_slots, max_pending
         cfg.max_pixels, cfg.lut_len, cfg.max_labels = max_pixels, lut_len, max_labels
-        cfg.max_bricks, cfg.tiles_per_step = max_bricks, tiles_per_step
+        cfg.max_bricks, cfg.tiles_per_step, cfg.evict_idle = max_bricks, tiles_per_step, int(bool(evict_idle))
         self.config = cfg
         h = C.c_void_p()
         capi._check(capi.lib().mk_server_create(C.byref(cfg), C.byref(h)), "mk_server_create")

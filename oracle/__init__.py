@@ -159,11 +159,17 @@ class RefGPU:
             L.mkref_render_kernel_ms.restype = C.c_double
             L.mkref_plane.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
             L.mkref_cpr.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int]
+            L.mkref_select.argtypes = [C.c_int]
             RefGPU._L = L
         self.L = RefGPU._L
 
     def device_count(self):
         return self.L.mkref_device_count()
+
+    def select(self, slot):
+        """Make resident volume slot 0..7 the one later calls use (slot 0
+        by default); each slot keeps its own volume, mask and LUTs."""
+        assert self.L.mkref_select(slot) == 0
 
     def set_volume(self, vox):
         self.vox = np.ascontiguousarray(vox, dtype=np.int16)

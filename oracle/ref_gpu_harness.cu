@@ -71,9 +71,23 @@ struct RefState {
     cudaTextureObjects tfs;
 };
 
-RefState g;
+// Several volumes can stay resident at once (the serving comparison runs
+// MonkeyGL's launchers over the same resident volumes as the server);
+// mkref_select chooses the one the other calls use.  MonkeyGL itself holds
+// one volume per process.
+constexpr int kRefSlots = 8;
+RefState g_slots[kRefSlots];
+RefState *g_cur = &g_slots[0];
 
 }  // namespace
+
+#define g (*g_cur)
+
+extern "C" int mkref_select(int slot) {
+    if (slot < 0 || slot >= kRefSlots) return 1;
+    g_cur = &g_slots[slot];
+    return 0;
+}
 
 // Flat VR parameter block (floats), in cu_render's argument order:
 //  [0..2] maxLenSpacing, [3..5] spacing, [6..8] spacingVoxel, [9] xT, [10] yT,

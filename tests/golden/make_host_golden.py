@@ -16,6 +16,7 @@ Writes tests/golden/host_geometry.json (scenarios and results).
 from __future__ import annotations
 
 import ctypes as C
+import os
 import json
 import sys
 from pathlib import Path
@@ -101,7 +102,11 @@ TF_CASES = [
 ]
 
 
-def main(ref_dir="/root/reference"):
+def main(ref_dir=None):
+    """ref_dir: the MonkeyGL source tree (argument, else $MONKEYGL_SRC)."""
+    ref_dir = ref_dir or os.environ.get("MONKEYGL_SRC")
+    if not ref_dir:
+        raise SystemExit("give the MonkeyGL source tree as an argument or in MONKEYGL_SRC")
     L = C.CDLL(str(LIB))
     vp = C.c_void_p
     L.mkrh_create.restype = vp

@@ -22,6 +22,7 @@ Writes tests/golden/overlay.npz.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import sys
 from pathlib import Path
 
@@ -39,7 +40,11 @@ CAMERAS = [(0, [])] + [(0, [(a, 0.0)]) for a in (10, 33, 45, 90, 137.5, 180, -60
 CPR_LINE = [[20.0 + 2.5 * i, 30.0 + 9.0 * np.sin(i / 3.0), 5.0 + 4.5 * i] for i in range(20)]
 
 
-def main(ref_dir="/root/reference"):
+def main(ref_dir=None):
+    """ref_dir: the MonkeyGL source tree (argument, else $MONKEYGL_SRC)."""
+    ref_dir = ref_dir or os.environ.get("MONKEYGL_SRC")
+    if not ref_dir:
+        raise SystemExit("give the MonkeyGL source tree as an argument or in MONKEYGL_SRC")
     L = C.CDLL(str(LIB))
     vp = C.c_void_p
     L.mkrh_create.restype = vp

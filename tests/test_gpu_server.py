@@ -159,3 +159,44 @@ def test_bad_requests_are_refused(vols):
         assert e.value.status == capi.MK_ERR_INVALID_ARGUMENT
         img, _ = srv.wait(srvmod.submit_request(srv, vid, vr))            # the server still works
         assert img.shape == (64, 64, 3)
+
+
+def test_eviction_under_a_budget_below_the_volumes(vols):
+    """evict_idle: with room for two of three volumes, adding the third
+    evicts the least recently used idle one, requests for an evicted volume
+    upload it again (evicting another), every image still equals the plain
+    path's, and the resident bytes never exceed the budget."""
+    third = make_phantom((72, 72, 56), (0.9, 0.9, 1.1), 33)
+    allv = [vols[0], vols[1], third]
+    with srvmod.Server(max_slots=3, max_pending=64, max_pixels=128 * 128, max_labels=8) as probe:
+        base = probe.stats()["resident_bytes"]
+        costs = []
+        for p in allv:
+            before = probe.stats()["resident_bytes"]
+            probe.add_volume(p.volume, p.labels)
+            costs.append(probe.stats()["resident_bytes"] - before)
+    budget = base + costs[0] + max(costs[1], costs[2]) + 4096
+    reqs = serving_trace(specs(allv), 36, 1000.0, seed=21, sizes=(48, 96))
+    plain = plain_images(allv, reqs)
+    with srvmod.Server(hbm_budget_bytes=budget, max_slots=3, max_pending=64, max_pixels=128 * 128, max_labels=8,
+                       evict_idle=True) as srv:
+        vids = [srv.add_volume(p.volume, p.labels) for p in allv]
+        st = srv.stats()
+        assert st["volumes"] == 3 and st["evictions"] >= 1 and st["resident_bytes"] <= budget
+        for rnd in range(2):
+            tickets = [srvmod.submit_request(srv, vids[r.volume], r) for r in reqs]
+            for i, t in enumerate(tickets):
+                img, _ = srv.wait(t)
+                assert np.array_equal(img, plain[i]), f"round {rnd} request {i} (volume {reqs[i].volume}) differs"
+                assert srv.stats()["resident_bytes"] <= budget
+        st = srv.stats()
+        print(f"evictions {st['evictions']}, loads {st['loads']}, resident {st['resident_bytes']} of {budget}")
+        assert st["loads"] >= 1 and st["evictions"] >= 2
+        # an evicted volume can be removed; one larger than the budget is refused
+        for v in vids:
+            srv.remove_volume(v)
+        assert srv.stats()["volumes"] == 0 and srv.stats()["resident_bytes"] == base
+        big = make_phantom((256, 256, 200), (1.0, 1.0, 1.0), 34)
+        with pytest.raises(capi.MonkeyGLError) as e:
+            srv.add_volume(big.volume)
+        assert e.value.status == capi.MK_ERR_BUDGET

@@ -43,6 +43,8 @@ def test_noalloc_cpr_matches_allocating_entry_point():
     for width, (pts, dirs), inv in calls:
         want = vol.render_cpr(width, pts, dirs, inv)
         out = torch.full((pts.shape[0], width), 12345, dtype=torch.int16, device="cuda")
+        # the fill is queued on torch's stream: the call's stream waits for it
+        stream.wait_stream(torch.cuda.current_stream())
         rc = _noalloc(vol, width, pts, dirs, inv, out, stream)
         assert rc == capi.MK_OK, capi.lib().mk_last_error()
         stream.synchronize()
@@ -63,4 +65,33 @@ def test_noalloc_cpr_rejects_paths_beyond_its_table():
     rc = _noalloc(vol, 8, pts, dirs, False, out, torch.cuda.Stream())
     assert rc == capi.MK_ERR_INVALID_ARGUMENT
     assert b"4096" in capi.lib().mk_last_error()
+    vol.close()
+
+
+def test_noalloc_cpr_leaves_device_memory_unchanged():
+    """After a first call on a new volume (which looks up the table's device
+    address), further calls of several path lengths must not change the
+    device's free memory: the entry point allocates nothing."""
+    import torch
+
+    w = wl.make_workload("small")
+    vol = capi.Volume(w.phantom.volume)
+    path = wl.vessel_path(w.phantom, rows=1000)
+    paths = [wl.cpr_straightened(path, 160), wl.cpr_stretched(path[:700], 200),
+             wl.cpr_straightened(path[:40], 64)]
+    stream = torch.cuda.Stream()
+    outs = [torch.zeros((p[0].shape[0], wd), dtype=torch.int16, device="cuda")
+            for p, wd in zip(paths, (160, 200, 64))]
+    stream.wait_stream(torch.cuda.current_stream())
+    assert _noalloc(vol, 160, *paths[0], False, outs[0], stream) == capi.MK_OK
+    stream.synchronize()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for rep in range(3):
+        for (pts, dirs), out in zip(paths, outs):
+            rc = _noalloc(vol, out.shape[1], pts, dirs, rep == 1, out, stream)
+            assert rc == capi.MK_OK, capi.lib().mk_last_error()
+    stream.synchronize()
+    free_after = torch.cuda.mem_get_info()[0]
+    assert free_after >= free_before, f"device free memory fell by {free_before - free_after} bytes"
     vol.close()
