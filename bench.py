@@ -70,6 +70,10 @@ def parse_args():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--saturation", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the serving and differentiable-rendering figures of the contract line")
+    ap.add_argument("--extra-requests", type=int, default=1000,
+                    help="requests of the contract line's serving trace")
     return ap.parse_args()
 
 
@@ -390,7 +394,37 @@ def run_mine(args, rank, local, world):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w, views[0], size, rtype)
     vol.close()
+    if rank == 0 and world == 1 and not args.no_extras and args.workload == "body":
+        line.update(extra_figures(args, w))
     return line
+
+
+def extra_figures(args, w):
+    """The metric's other figures, measured after the timed frames: served
+    p50/p99 latency and renders/s of the continuous-batching server against
+    this library's one-launch-per-request path (a short serving trace over
+    the four resident serving volumes), and the backward/forward time of the
+    differentiable renderer (256^3 float volume, 8 views of 256^2)."""
+    import torch
+    from monkeygl_b200 import serve_bench, suite
+    out = {}
+    sv = serve_bench.measure(n=args.extra_requests, rate=200.0, nsat=max(1, args.extra_requests // 2),
+                             phantoms=serve_bench.serving_phantoms(body=w.phantom), evict=False)
+    out["served_p50_ms"] = sv["server"]["p50_ms"]
+    out["served_p99_ms"] = sv["server"]["p99_ms"]
+    out["served_renders_per_s"] = sv["server"]["saturation_renders_per_s"]
+    out["plain_renders_per_s"] = sv["plain"]["saturation_renders_per_s"]
+    out["served_renders_per_s_ratio"] = sv["saturation_ratio"]
+    out["served_workload"] = (f"{args.extra_requests} requests (seeded Poisson 200/s; VR/MIP/MPR 60/20/20, "
+                              "256..1024^2, 4 resident volumes, random cameras and TFs); p50/p99 at the "
+                              "arrival rate, renders/s with the first half submitted at once; ratio against "
+                              "mk_render_vr/mk_render_plane one request per launch")
+    ctx = {"stream": torch.cuda.Stream(), "flush": torch.empty(256 << 20, dtype=torch.uint8, device="cuda")}
+    rows = suite.dvr_rows(ctx)
+    out["dvr_fwd_ms"] = rows[0]["ms"]
+    out["dvr_bwd_ms"] = rows[1]["ms"]
+    out["dvr_bwd_fwd_ratio"] = rows[1]["bwd_over_fwd"]
+    return out
 
 
 # ----------------------------------------------------------------------
@@ -436,7 +470,18 @@ def run_reference(args, rank, world):
         return out
     crc = frames_crc32(ref_view, len(flats))
     value = K / dt
-    return {
+    extras = {}
+    if args.workload == "body" and not args.no_extras:
+        from monkeygl_b200 import serve_bench
+        sv = serve_bench.measure_monkeygl(ref, n=args.extra_requests, rate=200.0,
+                                          nsat=max(1, args.extra_requests // 2),
+                                          phantoms=serve_bench.serving_phantoms(body=w.phantom))
+        extras = {"served_p50_ms": sv["p50_ms"], "served_p99_ms": sv["p99_ms"],
+                  "served_renders_per_s": sv["saturation_renders_per_s"],
+                  "served_workload": "the same trace as this line's other arm, one request per launch through "
+                                     "MonkeyGL's cu_setTransferFunc + cu_render / cu_renderPlane_* (volumes "
+                                     "resident in the harness)"}
+    line = {
         "metric": METRIC, "impl": "reference", "value": round(value, 3), "unit": "fps", "n_gpus": 1,
         "steps": K, "warmup": W, "ms_per_step": round(dt * 1e3 / K, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -451,6 +496,8 @@ def run_reference(args, rank, world):
                                    "CPU rendering path"},
         "clocks": {k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons", "samples")},
     }
+    line.update(extras)
+    return line
 
 
 def main():

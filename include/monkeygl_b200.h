@@ -365,6 +365,36 @@ int mk_merge_orientation_box(mk_mesh mesh, const float rotate[9], uint8_t *rgb, 
 int mk_draw_line_rgb(uint8_t *rgb, int width, int height, float x0, float y0, float x1, float y1,
                      int line_width, const float color[3]);
 
+/* PNG + Base64, the output form of MonkeyGL's GetVRData_pngString and
+ * GetPlaneData_pngString (core/HelloMonkey.cpp:212-259, 333-413, which use
+ * fpng): an 8-bit PNG of `channels` = 3 (RGB) or 4 (RGBA; MonkeyGL packs an
+ * int16 plane of width W as W/2 RGBA pixels) compressed in parallel row
+ * bands, then Base64, NUL-terminated, into `out` (`capacity` bytes, at least
+ * mk_encoded_capacity).  The decoded pixels equal the input; the bytes are
+ * not fpng's. */
+int mk_encoded_capacity(int width, int height, int channels, size_t *bytes);
+int mk_encode_png_base64(const uint8_t *pixels, int width, int height, int channels, char *out,
+                         size_t capacity, size_t *length);
+
+/* Text annotations (core/AnnotationLayer.cpp:41-61 ->
+ * AnnotationUtils::Textout2Image, core/AnnotationUtils.cpp:419-458).  The
+ * glyph masks are loaded from a glyph file ("MKGLYPH1": uint32 count, then per
+ * glyph uint8 font size 0..2, uint8 key length, the key bytes, uint16 width,
+ * uint16 height, width*height mask bytes); MonkeyGL's own masks are
+ * extracted into such a file by the oracle build (oracle/make_glyphs.py).
+ * The text is drawn byte by byte: a byte without a glyph moves the pen back
+ * one pixel and draws nothing; mask m > 0 sets each channel to the truncated
+ * m * colour; format 0 left, 1 right, 2 centred on x (MonkeyGL's
+ * AnnotationFormat); images below 10x10 are refused. */
+typedef struct mk_font_s *mk_font;
+int mk_font_load(const char *path, mk_font *out);
+int mk_font_destroy(mk_font font);
+/* AnnotationUtils::GetSize: total width (unknown bytes count -1) and the
+ * height of the last glyph. */
+int mk_text_size(mk_font font, const char *text, int font_size, int *width, int *height);
+int mk_draw_text_rgb(mk_font font, uint8_t *rgb, int width, int height, const char *text, int x, int y,
+                     int font_size, int format, const float color[3]);
+
 /* ------------------------------------------------------------------ */
 /* Serving: continuous batching of VR/MIP/MPR requests                 */
 /* ------------------------------------------------------------------ */
@@ -414,12 +444,18 @@ typedef struct mk_request {
     int n_luts;                  /* 0..max_labels; labels without a table are transparent */
     const float *label_params;   /* n_luts rows of (alpha, ww, wl), ww > 0; others (0, 1, 0) */
     void *out;                   /* host image: W*H*3 (RGB8) or *4 (RGBA8) bytes, W*H int16 for MPR */
+    char *encoded;               /* optional (NULL: none): also the image as MonkeyGL's *_pngString form,
+                                    a NUL-terminated Base64 PNG (mk_encode_png_base64; an MPR plane as
+                                    W/2 RGBA pixels, W even), written by the server's encoder thread
+                                    while later steps run; mk_server_wait returns once it is written */
+    size_t encoded_capacity;     /* bytes at `encoded`: at least mk_encoded_capacity of the image */
 } mk_request;
 
 typedef struct mk_request_times {
     double submitted_ms;         /* on the server's clock (ms since mk_server_create) */
     double started_ms;           /* first step holding its tiles was launched */
-    double completed_ms;         /* image copied to `out` */
+    double completed_ms;         /* image copied to `out` (and encoded, if asked for) */
+    size_t encoded_length;       /* characters written to `encoded` (0: not asked for) */
 } mk_request_times;
 
 typedef struct mk_server_stats {

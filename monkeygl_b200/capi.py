@@ -96,11 +96,13 @@ class Request(C.Structure):
     _fields_ = [
         ("volume", C.c_int), ("kind", C.c_int), ("vr", VRParams), ("plane", PlaneParams),
         ("luts", C.c_void_p), ("n_luts", C.c_int), ("label_params", C.c_void_p), ("out", C.c_void_p),
+        ("encoded", C.c_void_p), ("encoded_capacity", C.c_size_t),
     ]
 
 
 class RequestTimes(C.Structure):
-    _fields_ = [("submitted_ms", C.c_double), ("started_ms", C.c_double), ("completed_ms", C.c_double)]
+    _fields_ = [("submitted_ms", C.c_double), ("started_ms", C.c_double), ("completed_ms", C.c_double),
+                ("encoded_length", C.c_size_t)]
 
 
 class ServerStats(C.Structure):
@@ -143,6 +145,14 @@ _SIGS = {
     "mk_merge_orientation_box": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]),
     "mk_draw_line_rgb": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                    C.c_int, C.c_void_p]),
+    "mk_encoded_capacity": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+    "mk_encode_png_base64": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_size_t,
+                                       C.POINTER(C.c_size_t)]),
+    "mk_font_load": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "mk_font_destroy": (C.c_int, [C.c_void_p]),
+    "mk_text_size": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "mk_draw_text_rgb": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_int,
+                                   C.c_int, C.c_int, C.c_void_p]),
     "mk_render_cpr_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                         C.c_void_p, C.c_void_p]),
     "mk_volume_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),

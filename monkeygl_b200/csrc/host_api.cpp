@@ -2,8 +2,8 @@
 // over the per-instance engine and the C ABI.  Method by method this follows
 // core/HelloMonkey.cpp, core/IRender.cpp and core/Render.cpp; the outputs of
 // GetVRData / GetPlaneData come from the sm_100a kernels.  PNG output is
-// written with zlib (MonkeyGL uses fpng): the decoded pixels are the same,
-// the compressed bytes are not.
+// written by host_encode.cpp (zlib in parallel bands; MonkeyGL uses fpng):
+// the decoded pixels are the same, the compressed bytes are not.
 #include <zlib.h>
 
 #include <cstdio>
@@ -11,6 +11,7 @@
 
 #include "../../include/monkeygl/HelloMonkey.h"
 #include "../../include/monkeygl/IRender.h"
+#include "host_encode.h"
 #include "host_engine.h"
 
 namespace MonkeyGL {
@@ -19,79 +20,7 @@ namespace {
 
 LogLevel g_log_level = LogLevelWarn;
 
-void put_be32(std::vector<uint8_t> &v, uint32_t x) {
-    v.push_back(x >> 24);
-    v.push_back((x >> 16) & 0xff);
-    v.push_back((x >> 8) & 0xff);
-    v.push_back(x & 0xff);
-}
-
-void put_chunk(std::vector<uint8_t> &png, const char *type, const uint8_t *data, size_t n) {
-    put_be32(png, (uint32_t)n);
-    const size_t start = png.size();
-    png.insert(png.end(), type, type + 4);
-    if (n) png.insert(png.end(), data, data + n);
-    uLong crc = crc32(0L, Z_NULL, 0);
-    crc = crc32(crc, png.data() + start, (uInt)(png.size() - start));
-    put_be32(png, (uint32_t)crc);
-}
-
 }  // namespace
-
-// 8-bit PNG (colour type 2 for 3 channels, 6 for 4), filter 0 on every row.
-std::vector<uint8_t> EncodePNG(const uint8_t *pixels, int w, int h, int channels) {
-    std::vector<uint8_t> png;
-    if (!pixels || w <= 0 || h <= 0 || (channels != 3 && channels != 4)) return png;
-    static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
-    png.insert(png.end(), sig, sig + 8);
-    uint8_t ihdr[13];
-    const uint32_t be[2] = {(uint32_t)w, (uint32_t)h};
-    for (int i = 0; i < 2; ++i) {
-        ihdr[4 * i] = be[i] >> 24;
-        ihdr[4 * i + 1] = (be[i] >> 16) & 0xff;
-        ihdr[4 * i + 2] = (be[i] >> 8) & 0xff;
-        ihdr[4 * i + 3] = be[i] & 0xff;
-    }
-    ihdr[8] = 8;
-    ihdr[9] = channels == 3 ? 2 : 6;
-    ihdr[10] = ihdr[11] = ihdr[12] = 0;
-    put_chunk(png, "IHDR", ihdr, 13);
-    const size_t row = (size_t)w * channels;
-    std::vector<uint8_t> raw((row + 1) * h);
-    for (int y = 0; y < h; ++y) {
-        raw[y * (row + 1)] = 0;
-        std::memcpy(&raw[y * (row + 1) + 1], pixels + y * row, row);
-    }
-    uLongf clen = compressBound((uLong)raw.size());
-    std::vector<uint8_t> z(clen);
-    if (compress2(z.data(), &clen, raw.data(), (uLong)raw.size(), 1) != Z_OK) return std::vector<uint8_t>();
-    put_chunk(png, "IDAT", z.data(), clen);
-    put_chunk(png, "IEND", nullptr, 0);
-    return png;
-}
-
-std::string Base64Encode(const uint8_t *data, size_t n) {
-    static const char tbl[] = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
-    std::string out;
-    out.reserve(((n + 2) / 3) * 4);
-    size_t i = 0;
-    for (; i + 2 < n; i += 3) {
-        const uint32_t v = (data[i] << 16) | (data[i + 1] << 8) | data[i + 2];
-        out.push_back(tbl[v >> 18]);
-        out.push_back(tbl[(v >> 12) & 63]);
-        out.push_back(tbl[(v >> 6) & 63]);
-        out.push_back(tbl[v & 63]);
-    }
-    if (i < n) {
-        uint32_t v = data[i] << 16;
-        if (i + 1 < n) v |= data[i + 1] << 8;
-        out.push_back(tbl[v >> 18]);
-        out.push_back(tbl[(v >> 12) & 63]);
-        out.push_back(i + 1 < n ? tbl[(v >> 6) & 63] : '=');
-        out.push_back('=');
-    }
-    return out;
-}
 
 // ---------------------------------------------------------------------------
 // IRender: forwards to this instance's engine (core/IRender.cpp)
@@ -251,8 +180,8 @@ std::string HelloMonkey::GetPlaneData_pngString(const PlaneType &t) {
     int w = 0, h = 0;
     std::shared_ptr<short> p;
     if (!m_pRender->GetPlaneData(p, w, h, t) || !p) return "";
-    std::vector<uint8_t> png = EncodePNG(reinterpret_cast<uint8_t *>(p.get()), w / 2, h, 4);
-    return Base64Encode(png.data(), png.size());
+    std::vector<uint8_t> png = mk::encode_png(reinterpret_cast<uint8_t *>(p.get()), w / 2, h, 4);
+    return mk::base64_string(png.data(), png.size());
 }
 
 // Axial slice of the stored volume, voxels outside every object set to
@@ -270,8 +199,8 @@ std::string HelloMonkey::GetOriginData_pngString(int slice) {
         for (size_t i = 0; i < s.size(); ++i)
             if (m[i] == 0) s[i] = -2048;
     }
-    std::vector<uint8_t> png = EncodePNG(reinterpret_cast<uint8_t *>(s.data()), w / 2, h, 4);
-    return Base64Encode(png.data(), png.size());
+    std::vector<uint8_t> png = mk::encode_png(reinterpret_cast<uint8_t *>(s.data()), w / 2, h, 4);
+    return mk::base64_string(png.data(), png.size());
 }
 
 bool HelloMonkey::GetCrossHairPoint(double &x, double &y, const PlaneType &t) { return m_pRender->GetCrossHairPoint(x, y, t); }
@@ -301,11 +230,11 @@ std::vector<uint8_t> HelloMonkey::GetVRData_png(int, int) {
     m_pRender->GetVRSize(w, h);
     std::shared_ptr<unsigned char> p;
     if (!m_pRender->GetVRData(p, w, h) || !p) return std::vector<uint8_t>();
-    return EncodePNG(p.get(), w, h, 3);
+    return mk::encode_png(p.get(), w, h, 3);
 }
 std::string HelloMonkey::GetVRData_pngString() {
     std::vector<uint8_t> png = GetVRData_png(0, 0);
-    return Base64Encode(png.data(), png.size());
+    return mk::base64_string(png.data(), png.size());
 }
 void HelloMonkey::SaveVR2Png(const char *file, int w, int h) {
     std::vector<uint8_t> png = GetVRData_png(w, h);
@@ -376,7 +305,7 @@ void HelloMonkey::ShowPlaneInVR(bool b) { m_pRender->ShowPlaneInVR(b); }
 
 // Base64 of the first w*h bytes, printed as a quoted line (core/HelloMonkey.cpp:53-61)
 void HelloMonkey::Transfer2Base64(unsigned char *p, int w, int h) {
-    std::string s = Base64Encode(p, (size_t)w * h);
+    std::string s = mk::base64_string(p, (size_t)w * h);
     std::printf("\"%s\",\n", s.c_str());
 }
 

@@ -261,11 +261,15 @@ Engine::Engine() {
     // MarchingCube's constructor reads the orientation mesh relative to the
     // working directory (core/MarchingCube.cpp:298)
     if (mk_mesh_load_stl("./resources/human.stl", &mesh_) != MK_OK) mesh_ = nullptr;
+    // the annotation glyphs, from the same resource directory (no glyph
+    // file: annotations are kept but not drawn)
+    if (mk_font_load("./resources/annotation_glyphs.bin", &font_) != MK_OK) font_ = nullptr;
 }
 
 Engine::~Engine() {
     if (dev_) mk_volume_destroy(dev_);
     if (mesh_) mk_mesh_destroy(mesh_);
+    if (font_) mk_font_destroy(font_);
 }
 
 // ---- volume (DataManager.cpp:144-175, VolumeInfo.cpp:78-148) -------------
@@ -1219,6 +1223,15 @@ bool Engine::RenderVR(std::shared_ptr<unsigned char> &out, int &w, int &h) {
                     dst[3 * i + 1] = src[3 * i + 1];
                     dst[3 * i + 2] = src[3 * i + 2];
                 }
+        }
+    }
+    // AnnotationLayer::GetRGBData (core/AnnotationLayer.cpp:41-61): every VR
+    // annotation in the order added, on images larger than 10x10
+    if (LayerEnabled(LayerTypeAnnotation) && font_ && w > 10 && h > 10) {
+        for (const Annotation &a : annotations_) {
+            if (a.plane != PlaneVR || a.format < AnnotationFormatLeft) continue;
+            const float clr[3] = {a.color.red, a.color.green, a.color.blue};
+            mk_draw_text_rgb(font_, out.get(), w, h, a.text.c_str(), a.x, a.y, (int)a.size, (int)a.format, clr);
         }
     }
     if (LayerEnabled(LayerTypeCPRLine) && cprLine_.size() >= 2) {

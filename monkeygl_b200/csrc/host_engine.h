@@ -222,6 +222,7 @@ private:
     // orientation box mesh (./resources/human.stl at construction, as
     // MonkeyGL's MarchingCube loads it); null when the file is absent
     mk_mesh mesh_ = nullptr;
+    mk_font font_ = nullptr;          // annotation glyphs (./resources/annotation_glyphs.bin)
 
     // device
     mk_volume dev_ = nullptr;

@@ -446,3 +446,136 @@ extern "C" int mk_draw_line_rgb(uint8_t *rgb, int width, int height, float x0, f
     });
     return MK_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Text annotations.  MonkeyGL draws VR annotations from 8-bit glyph masks of
+// three font sizes (core/AnnotationUtils.cpp:42-376) with
+// AnnotationUtils::Textout2Image (core/AnnotationUtils.cpp:419-458).  The
+// masks are not part of this library: a glyph file (format below) supplies
+// them, and the drawing follows Textout2Image:
+//   - the text is taken one byte at a time; a byte without a glyph counts as
+//     a glyph of width -1 and height -1 (nothing drawn, the pen moves back one
+//     pixel), as MonkeyGL's map lookup of an unknown character gives;
+//   - right / centred text starts the total width (sum of the widths, the
+//     height of the last glyph) / half of it (integer division) to the left;
+//   - a glyph pixel with mask m > 0 inside the image becomes m * colour in
+//     each channel, converted to 8 bits by truncation;
+//   - nothing is drawn into images of width or height below 10.
+// Glyph file: "MKGLYPH1", uint32 count, then per glyph: uint8 font size
+// (0 small, 1 middle, 2 big), uint8 key length, the key bytes (the
+// character), uint16 width, uint16 height, width * height mask bytes.
+struct mk_font_s {
+    struct Glyph {
+        int w = -1, h = -1;
+        std::vector<uint8_t> mask;
+    };
+    std::unordered_map<std::string, Glyph> glyphs[3];
+};
+
+namespace {
+
+const mk_font_s::Glyph &font_glyph(const mk_font_s *f, int size, char c) {
+    static const mk_font_s::Glyph unknown;
+    if (size < 0 || size > 2) return unknown;
+    auto it = f->glyphs[size].find(std::string(1, c));
+    return it == f->glyphs[size].end() ? unknown : it->second;
+}
+
+// float -> 8 bits as an x86 build of MonkeyGL's assignment converts it
+// (truncation to a 32-bit integer, then its low byte)
+inline uint8_t to_u8(float v) { return (uint8_t)(int32_t)v; }
+
+}  // namespace
+
+extern "C" int mk_font_load(const char *path, mk_font *out) {
+    if (!path || !out) {
+        set_err("mk_font_load: null argument");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    FILE *fp = fopen(path, "rb");
+    if (!fp) {
+        set_err(std::string("mk_font_load: cannot open ") + path);
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    std::unique_ptr<mk_font_s> f(new mk_font_s());
+    char magic[8];
+    uint32_t n = 0;
+    bool ok = fread(magic, 1, 8, fp) == 8 && memcmp(magic, "MKGLYPH1", 8) == 0 && fread(&n, 4, 1, fp) == 1 &&
+              n <= 4096;
+    for (uint32_t i = 0; ok && i < n; ++i) {
+        uint8_t size = 0, klen = 0;
+        uint16_t w = 0, h = 0;
+        char key[256];
+        ok = fread(&size, 1, 1, fp) == 1 && fread(&klen, 1, 1, fp) == 1 && size <= 2 && klen > 0 &&
+             fread(key, 1, klen, fp) == klen && fread(&w, 2, 1, fp) == 1 && fread(&h, 2, 1, fp) == 1;
+        if (!ok) break;
+        mk_font_s::Glyph g;
+        g.w = w;
+        g.h = h;
+        g.mask.resize((size_t)w * h);
+        ok = g.mask.empty() || fread(g.mask.data(), 1, g.mask.size(), fp) == g.mask.size();
+        if (ok) f->glyphs[size][std::string(key, klen)] = std::move(g);
+    }
+    fclose(fp);
+    if (!ok) {
+        set_err(std::string("mk_font_load: malformed glyph file ") + path);
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    *out = f.release();
+    return MK_OK;
+}
+
+extern "C" int mk_font_destroy(mk_font font) {
+    if (!font) return MK_ERR_INVALID_ARGUMENT;
+    delete font;
+    return MK_OK;
+}
+
+extern "C" int mk_text_size(mk_font font, const char *text, int font_size, int *width, int *height) {
+    if (!font || !text || !width || !height) {
+        set_err("mk_text_size: null argument");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    // AnnotationUtils::GetSize (core/AnnotationUtils.cpp:460-470)
+    int w = 0, h = 0;
+    for (const char *c = text; *c; ++c) {
+        const mk_font_s::Glyph &g = font_glyph(font, font_size, *c);
+        w += g.w;
+        h = g.h;
+    }
+    *width = w;
+    *height = h;
+    return MK_OK;
+}
+
+extern "C" int mk_draw_text_rgb(mk_font font, uint8_t *rgb, int width, int height, const char *text, int x, int y,
+                                int font_size, int format, const float color[3]) {
+    if (!font || !rgb || !text || !color || width < 10 || height < 10 || format < 0 || format > 2) {
+        set_err("mk_draw_text_rgb: bad arguments (image of at least 10x10, format 0..2)");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    int x0 = x;
+    if (format != 0) {                                 // AnnotationFormatRight = 1, Center = 2
+        int w = 0, h = 0;
+        mk_text_size(font, text, font_size, &w, &h);
+        x0 -= format == 2 ? w / 2 : w;
+    }
+    for (const char *c = text; *c; ++c) {
+        const mk_font_s::Glyph &g = font_glyph(font, font_size, *c);
+        for (int yy = y; yy < y + g.h; ++yy) {
+            if (yy < 0 || yy >= height) continue;
+            for (int xx = x0; xx < x0 + g.w; ++xx) {
+                if (xx < 0 || xx >= width) continue;
+                const uint8_t m = g.mask[(size_t)(yy - y) * g.w + (xx - x0)];
+                if (m == 0) continue;
+                uint8_t *p = rgb + 3 * ((size_t)yy * width + xx);
+                p[0] = to_u8(m * color[0]);
+                p[1] = to_u8(m * color[1]);
+                p[2] = to_u8(m * color[2]);
+            }
+        }
+        x0 += g.w;
+    }
+    return MK_OK;
+}

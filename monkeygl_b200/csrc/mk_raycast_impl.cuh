@@ -594,7 +594,13 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             const bool pos_a = aj > 0.0f;
             const bool refine_j = pos_a && busy && Q.step != L8;
             const bool stop_j = !pos_a || Q.step == L4 || (Q.step == L1 ? busy : !busy);
-            const bool plain_j = (flags & (kCoopEnd | kCoopOutside | kCoopFetched)) == kCoopFetched;
+            // A sample in a skippable empty brick (coarse step, not fetched)
+            // counts as a fetched sample of alpha 0: where the walk reaches
+            // it after an alpha <= 0.001 it skips it with aPre = 0 and no
+            // step change, exactly what an alpha-0 sample gives; after a
+            // larger alpha the walk has already stopped at the sample before.
+            const bool plain_j = (flags & (kCoopEnd | kCoopOutside)) == 0 &&
+                                 (flags & (kCoopFetched | kCoopEmpty)) != 0;
             const unsigned plain_m = __ballot_sync(FULL, plain_j);
             const unsigned stop_m = __ballot_sync(FULL, stop_j);
             const unsigned refine_m = __ballot_sync(FULL, refine_j);
@@ -613,6 +619,14 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     pre_out = alpha_j;
                     step_out = Q.step;
                     lat_out = Q.lat >= 0 ? Q.lat + G : Q.lat;
+                    if ((flags & (kCoopEmpty | kCoopFetched)) == kCoopEmpty && nskip > 0) {
+                        // the last sample starts a skip: the walk jumps to the
+                        // end of its empty brick from here
+                        lat_out = Q.lat >= 0 ? Q.lat + j : -1;
+                        a_out = aj;
+                        advance_coarse(P, a_out, lat_out, Q.step, 1 + nskip);
+                        pre_out = 0.0f;
+                    }
                 } else if (refine_j) {              // refine before compositing sample j
                     a_out = Q.step == L1 ? aj - (L1 - L4) : aj - (L4 - L8);
                     pre_out = pre_j;

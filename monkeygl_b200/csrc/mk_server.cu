@@ -41,6 +41,7 @@
 #include <thread>
 #include <vector>
 
+#include "host_encode.h"
 #include "mk_internal.h"
 #include "mk_math.h"
 #include "mk_raycast_impl.cuh"
@@ -167,6 +168,8 @@ struct Req {
     std::shared_ptr<const std::vector<int>> order;   // tile order (ray casting: centre first)
     size_t out_bytes = 0;
     bool direct = false;
+    int enc_w = 0, enc_h = 0, enc_ch = 0;   // encoded form: PNG geometry (enc_ch 0: none)
+    size_t enc_len = 0;
     bool done = false;
     int status = MK_OK;
     double t_submit = 0, t_start = -1, t_done = 0;
@@ -216,6 +219,10 @@ struct mk_server_s {
     std::deque<int> load_queue;
     std::condition_variable cv_load;
     std::thread loader;
+    // requests whose image waits for its PNG + Base64 form
+    std::deque<uint64_t> enc_queue;
+    std::condition_variable cv_enc;
+    std::thread encoder;
     mk_server_stats stats;
     bool stop = false;
     int fatal = MK_OK;
@@ -462,8 +469,13 @@ void worker_loop(mk_server_s *s) {
             const double now = s->now_ms();
             for (uint64_t t : st.finishing) {
                 Req &q = s->reqs[t];
-                q.done = true;
-                q.t_done = now;
+                if (q.enc_ch) {
+                    s->enc_queue.push_back(t);        // done once the encoder has written its form
+                    s->cv_enc.notify_one();
+                } else {
+                    q.done = true;
+                    q.t_done = now;
+                }
                 s->slots[q.slot].ticket = 0;
                 s->active.erase(std::find(s->active.begin(), s->active.end(), t));
                 auto it = s->volumes.find(q.r.volume);
@@ -534,6 +546,47 @@ void worker_loop(mk_server_s *s) {
                 s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
             }
         }
+    }
+}
+
+// Writes the PNG + Base64 form of finished requests that asked for it (the
+// image is already in the request's host buffer), one request at a time with
+// the encoder's parallel bands, while the worker runs later steps.
+void encoder_loop(mk_server_s *s) {
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        if (s->enc_queue.empty()) {
+            if (s->stop && s->pending.empty() && s->active.empty() && s->inflight.empty()) break;
+            s->cv_enc.wait_for(lk, std::chrono::milliseconds(20));
+            continue;
+        }
+        const uint64_t t = s->enc_queue.front();
+        s->enc_queue.pop_front();
+        auto it = s->reqs.find(t);
+        if (it == s->reqs.end() || it->second.done) continue;   // failed meanwhile
+        const Req &q = it->second;
+        const uint8_t *img = static_cast<const uint8_t *>(q.r.out);
+        const int w = q.enc_w, h = q.enc_h, ch = q.enc_ch;
+        char *dst = q.r.encoded;
+        const size_t cap = q.r.encoded_capacity;
+        lk.unlock();
+        const std::vector<uint8_t> png = encode_png(img, w, h, ch);
+        size_t n = 0;
+        int st = MK_OK;
+        if (png.empty() || ((png.size() + 2) / 3) * 4 + 1 > cap) {
+            st = MK_ERR_OUT_OF_MEMORY;
+        } else {
+            n = base64_encode(png.data(), png.size(), dst);
+            dst[n] = '\0';
+        }
+        lk.lock();
+        auto jt = s->reqs.find(t);          // a failure meanwhile may have completed (and freed) it
+        if (jt == s->reqs.end() || jt->second.done) continue;
+        jt->second.enc_len = n;
+        jt->second.status = st;
+        jt->second.done = true;
+        jt->second.t_done = s->now_ms();
+        s->cv_done.notify_all();
     }
 }
 
@@ -810,6 +863,7 @@ extern "C" int mk_server_create(const mk_server_config *config, mk_server *out) 
     s->stats.budget_bytes = s->budget;
     s->t0 = Clock::now();
     s->worker = std::thread(worker_loop, s);
+    s->encoder = std::thread(encoder_loop, s);
     if (c.evict_idle) s->loader = std::thread(loader_loop, s);
     *out = s;
     return MK_OK;
@@ -825,6 +879,8 @@ extern "C" int mk_server_destroy(mk_server s) {
     if (s->worker.joinable()) s->worker.join();
     s->cv_load.notify_all();
     if (s->loader.joinable()) s->loader.join();
+    s->cv_enc.notify_all();
+    if (s->encoder.joinable()) s->encoder.join();
     cudaSetDevice(s->cfg.device);
     cudaStreamSynchronize(s->stream);
     cudaStreamSynchronize(s->step_stream[0]);
@@ -968,6 +1024,15 @@ extern "C" int mk_server_submit(mk_server s, const mk_request *req, uint64_t *ti
         q.tiles_x = (P.W + 31) / 32;
         q.tiles_total = q.tiles_x * ((P.H + 7) / 8);
         q.out_bytes = (size_t)P.W * P.H * sizeof(int16_t);
+        if (req->encoded) {
+            if (P.W % 2) {
+                set_last_error("mk_server_submit: an encoded plane needs an even width");
+                return MK_ERR_INVALID_ARGUMENT;
+            }
+            q.enc_w = P.W / 2;                // MonkeyGL's packing: 2 int16 per RGBA pixel
+            q.enc_h = P.H;
+            q.enc_ch = 4;
+        }
     } else if (req->kind >= MK_REQUEST_VR && req->kind <= MK_REQUEST_SURFACE) {
         mk_vr_params vp = req->vr;
         vp.render_type = req->kind;
@@ -993,6 +1058,11 @@ extern "C" int mk_server_submit(mk_server s, const mk_request *req, uint64_t *ti
         q.tiles_x = (P.W + 31) / 32;
         q.tiles_total = q.tiles_x * ((P.H + 7) / 8);
         q.out_bytes = (size_t)P.W * P.H * (P.rgba ? 4 : 3);
+        if (req->encoded) {
+            q.enc_w = P.W;
+            q.enc_h = P.H;
+            q.enc_ch = P.rgba ? 4 : 3;
+        }
         const std::array<int, 4> key = {P.W, P.H, (int)lrintf(P.xT), (int)lrintf(P.yT)};
         auto oit = s->orders.find(key);
         if (oit == s->orders.end()) {
@@ -1003,6 +1073,10 @@ extern "C" int mk_server_submit(mk_server s, const mk_request *req, uint64_t *ti
         q.order = oit->second;
     } else {
         set_last_error("mk_server_submit: unknown request kind");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    if (q.enc_ch && req->encoded_capacity < encoded_capacity(q.enc_w, q.enc_h, q.enc_ch)) {
+        set_last_error("mk_server_submit: encoded_capacity below mk_encoded_capacity of the image");
         return MK_ERR_INVALID_ARGUMENT;
     }
     if ((int)s->pending.size() >= s->cfg.max_pending) {
@@ -1043,6 +1117,7 @@ extern "C" int mk_server_wait(mk_server s, uint64_t ticket, int timeout_ms, mk_r
         times->submitted_ms = q.t_submit;
         times->started_ms = q.t_start;
         times->completed_ms = q.t_done;
+        times->encoded_length = q.enc_len;
     }
     const int st = q.status;
     if (st != MK_OK) set_last_error(s->fatal_msg);

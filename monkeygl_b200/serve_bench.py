@@ -125,7 +125,8 @@ def run_monkeygl(ref, trace, pool, open_loop: bool):
     (an array allocated per table), then cu_render (output allocated, kernel,
     synchronous copy, free) or cu_renderPlane_*.  The volumes stay resident
     in the harness's slots, which MonkeyGL's one-volume singleton cannot do,
-    so no upload is counted."""
+    so no upload is counted.  Volume i of the trace is the harness's slot
+    i + 1 (slot 0 keeps the volume its caller loaded)."""
     from . import capi
     b = pool.take()
     lat = []
@@ -136,7 +137,7 @@ def run_monkeygl(ref, trace, pool, open_loop: bool):
             dt = t0 + r.arrival_s - time.perf_counter()
             if dt > 0:
                 time.sleep(dt)
-        ref.select(r.volume)
+        ref.select(r.volume + 1)
         if r.kind == capi.REQUEST_MPR:
             ref.plane(r.size, r.size, capi.plane_params_flat(r.plane), r.plane.mpr_type, r.plane.sampling)
         else:
@@ -154,7 +155,7 @@ def run_monkeygl(ref, trace, pool, open_loop: bool):
     return lat, wall
 
 
-def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True, log=None):
+def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True):
     """The serving figures as a dict: the trace through the server, through
     this library's one-launch-per-request path and (with `ref`, MonkeyGL's
     kernels) through MonkeyGL's one-launch-per-request path; then an
@@ -164,13 +165,12 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True,
     import torch
     from . import capi
     from . import server as S
-    from .phantom import make_phantom
-    from .workloads import SERVING_VOLUMES, serving_trace
+    from .workloads import serving_trace
 
     nsat = min(n, nsat)
     torch.cuda.init()
     if phantoms is None:
-        phantoms = [make_phantom(d, s, seed, with_labels=lab) for d, s, seed, lab in SERVING_VOLUMES]
+        phantoms = serving_phantoms()
     specs = [(p.dims, p.spacing, p.labels is not None) for p in phantoms]
     trace = serving_trace(specs, n, rate, seed=2024)
     pool = _Pool(64, 1024 * 1024 * 4)
@@ -238,7 +238,7 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True,
     line["saturation_latency"] = {"server": _pcts(sat_s_lat), "plain": _pcts(sat_p_lat)}
     if ref is not None:
         for i, p in enumerate(phantoms):
-            ref.select(i)
+            ref.select(i + 1)
             ref.set_volume(p.volume)
             ref.set_mask(p.labels)
         lat_m, wall_m = run_monkeygl(ref, trace, pool, open_loop=True)
@@ -263,6 +263,42 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True,
                             "volumes_mb": round(sum(vol_bytes) / 2 ** 20, 1),
                             "evictions": est["evictions"], "loads": est["loads"]}
     return line
+
+
+def serving_phantoms(body=None):
+    """The four serving phantoms (workloads.SERVING_VOLUMES); `body` may pass
+    the 512x512x1559 labelled one (the same seed as the body workload)."""
+    from .phantom import make_phantom
+    from .workloads import SERVING_VOLUMES
+    out = []
+    for d, sp, seed, lab in SERVING_VOLUMES:
+        if body is not None and tuple(d) == tuple(body.dims) and lab and seed == 1236:
+            out.append(body)
+        else:
+            out.append(make_phantom(d, sp, seed, with_labels=lab))
+    return out
+
+
+def measure_monkeygl(ref, n=1000, rate=200.0, nsat=500, phantoms=None):
+    """MonkeyGL's one-launch-per-request path alone on the same trace as
+    measure(): p50/p99 at the arrival rate and renders/s at saturation."""
+    from .workloads import serving_trace
+    if phantoms is None:
+        phantoms = serving_phantoms()
+    specs = [(p.dims, p.spacing, p.labels is not None) for p in phantoms]
+    trace = serving_trace(specs, n, rate, seed=2024)
+    nsat = min(n, nsat)
+    pool = _Pool(2, 1024 * 1024 * 4)
+    for i, p in enumerate(phantoms):
+        ref.select(i + 1)
+        ref.set_volume(p.volume)
+        ref.set_mask(p.labels)
+    run_monkeygl(ref, serving_trace(specs, 64, 1000.0, seed=99), pool, open_loop=False)   # warm-up
+    lat, wall = run_monkeygl(ref, trace, pool, open_loop=True)
+    _, sat = run_monkeygl(ref, trace[:nsat], pool, open_loop=False)
+    ref.select(0)
+    return {**_pcts(lat), "renders_per_s": round(n / wall, 1), "saturation_renders_per_s": round(nsat / sat, 1),
+            "requests": n, "saturation_requests": nsat}
 
 
 def main(args, ref=None):

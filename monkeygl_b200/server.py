@@ -81,17 +81,26 @@ class Server:
         capi._check(capi.lib().mk_server_remove_volume(self.handle, vid), "mk_server_remove_volume")
         self._dims.pop(vid, None)
 
-    def _submit(self, req: capi.Request, out, keep) -> int:
+    def _submit(self, req: capi.Request, out, keep, encode=None) -> int:
+        """encode: None, or (width, height, channels) of the PNG to also produce."""
         t = C.c_uint64(0)
         req.out = out.ctypes.data
+        enc = None
+        if encode is not None:
+            cap = C.c_size_t(0)
+            capi._check(capi.lib().mk_encoded_capacity(*encode, C.byref(cap)), "mk_encoded_capacity")
+            enc = np.zeros(cap.value, np.uint8)
+            req.encoded = enc.ctypes.data
+            req.encoded_capacity = cap.value
         capi._check(capi.lib().mk_server_submit(self.handle, C.byref(req), C.byref(t)), "mk_server_submit")
-        self._outs[t.value] = (out, keep)
+        self._outs[t.value] = (out, (keep, enc))
         return t.value
 
     def submit_vr(self, vid: int, params: capi.VRParams, luts, label_params, kind: int = capi.REQUEST_VR,
-                  out: np.ndarray | None = None) -> int:
+                  out: np.ndarray | None = None, encode: bool = False) -> int:
         """Ray-cast request.  luts: (n, lut_len, 4) float32 for labels 0..n-1;
-        label_params: (n, 3) rows of (alpha, ww, wl)."""
+        label_params: (n, 3) rows of (alpha, ww, wl).  encode: also return
+        the image as a Base64 PNG (times["png_base64"] from wait)."""
         lt = np.ascontiguousarray(luts, dtype=np.float32)
         if lt.ndim == 2:
             lt = lt[None]
@@ -108,15 +117,18 @@ class Server:
         keep = None
         if out is None:
             out, keep = _pinned_empty((params.height, params.width, ch), np.uint8)
-        return self._submit(req, out, keep)
+        return self._submit(req, out, keep, (params.width, params.height, ch) if encode else None)
 
-    def submit_plane(self, vid: int, params: capi.PlaneParams, out: np.ndarray | None = None) -> int:
+    def submit_plane(self, vid: int, params: capi.PlaneParams, out: np.ndarray | None = None,
+                     encode: bool = False) -> int:
+        """MPR request; encode: also the plane as MonkeyGL's Base64 PNG (W/2
+        RGBA pixels, even widths only)."""
         req = capi.Request()
         req.volume, req.kind, req.plane = vid, capi.REQUEST_MPR, params
         keep = None
         if out is None:
             out, keep = _pinned_empty((params.height, params.width), np.int16)
-        return self._submit(req, out, keep)
+        return self._submit(req, out, keep, (params.width // 2, params.height, 4) if encode else None)
 
     def wait(self, ticket: int, timeout_ms: int = -1):
         """(image, times) once the request is done; raises MonkeyGLError with
@@ -125,9 +137,12 @@ class Server:
         rc = capi.lib().mk_server_wait(self.handle, C.c_uint64(ticket), int(timeout_ms), C.byref(tm))
         if rc == capi.MK_ERR_TIMEOUT:
             raise capi.MonkeyGLError(rc, "mk_server_wait")
-        out, _ = self._outs.pop(ticket)
+        out, (_, enc) = self._outs.pop(ticket)
         capi._check(rc, "mk_server_wait")
-        return out, {"submitted_ms": tm.submitted_ms, "started_ms": tm.started_ms, "completed_ms": tm.completed_ms}
+        times = {"submitted_ms": tm.submitted_ms, "started_ms": tm.started_ms, "completed_ms": tm.completed_ms}
+        if enc is not None:
+            times["png_base64"] = enc[:tm.encoded_length].tobytes().decode("ascii")
+        return out, times
 
     def stats(self) -> dict:
         st = capi.ServerStats()
@@ -135,11 +150,11 @@ class Server:
         return {k: getattr(st, k) for k, _ in capi.ServerStats._fields_}
 
 
-def submit_request(srv: Server, vid: int, req, out: np.ndarray | None = None) -> int:
+def submit_request(srv: Server, vid: int, req, out: np.ndarray | None = None, encode: bool = False) -> int:
     """Submit a workloads.ServingRequest for volume id `vid`."""
     if req.kind == capi.REQUEST_MPR:
-        return srv.submit_plane(vid, req.plane, out=out)
-    return srv.submit_vr(vid, req.vr, req.luts, req.label_params, kind=req.kind, out=out)
+        return srv.submit_plane(vid, req.plane, out=out, encode=encode)
+    return srv.submit_vr(vid, req.vr, req.luts, req.label_params, kind=req.kind, out=out, encode=encode)
 
 
 def render_plain(vol: capi.Volume, req, out: np.ndarray | None = None) -> np.ndarray:

@@ -18,6 +18,7 @@
 
 #include <cuda_runtime.h>
 
+#include "AnnotationUtils.h"
 #include "CuDataManager.h"
 #include "DataManager.h"
 #include "Defines.h"
@@ -369,4 +370,46 @@ extern "C" void mkrh_rotate_matrix(float *out) {
 extern "C" void mkrh_draw_line(unsigned char *img, int w, int h, float x0, float y0, float x1, float y1, int lw,
                                float r, float g, float b) {
     Methods::DrawLineInImage24Bit(img, w, h, x0, y0, x1, y1, lw, RGBA(r, g, b));
+}
+
+// HelloMonkey::AddAnnotation / RemoveAllAnnotations (core/HelloMonkey.h:121-123).
+extern "C" int mkrh_add_annotation(void *h, const char *txt, int x, int y, int font_size, int format, float r,
+                                   float g, float b, float a) {
+    return HM->AddAnnotation(PlaneVR, std::string(txt), x, y, (FontSize)font_size, (AnnotationFormat)format,
+                             RGBA(r, g, b, a)) ? 1 : 0;
+}
+extern "C" int mkrh_remove_annotations(void *h) { return HM->RemoveAllAnnotations() ? 1 : 0; }
+
+// MonkeyGL's text rendering (core/AnnotationUtils.cpp:419-458) on an RGB image.
+extern "C" int mkrh_textout(const char *txt, int x, int y, int font_size, int format, float r, float g, float b,
+                            unsigned char *img, int w, int hh) {
+    static bool init = AnnotationUtils::Init();
+    (void)init;
+    AnnotationUtils::SetFontSize((FontSize)font_size);
+    return AnnotationUtils::Textout2Image(std::string(txt), x, y, (AnnotationFormat)format, RGBA(r, g, b), img, w,
+                                          hh) ? 1 : 0;
+}
+
+// The glyph mask MonkeyGL draws character `c` with at `font_size`: its size
+// from AnnotationUtils::GetSize and its mask values read back from a
+// Textout2Image call in white on black (pixel = mask * 1.0 where mask > 0).
+// Returns 1 with wh = (width, height) and the mask in out (row-major), 0 for
+// a character MonkeyGL has no glyph for.
+extern "C" int mkrh_glyph(const char *c, int font_size, unsigned char *out, int cap, int *wh) {
+    static bool init = AnnotationUtils::Init();
+    (void)init;
+    AnnotationUtils::SetFontSize((FontSize)font_size);
+    int w = -1, hh = -1;
+    AnnotationUtils::GetSize(std::string(c), w, hh);
+    wh[0] = w;
+    wh[1] = hh;
+    if (w <= 0 || hh <= 0 || w * hh > cap) return 0;
+    const int cw = w < 16 ? 16 : w, ch = hh < 16 ? 16 : hh;
+    std::vector<unsigned char> img((size_t)cw * ch * 3, 0);
+    if (!AnnotationUtils::Textout2Image(std::string(c), 0, 0, AnnotationFormatLeft, RGBA(1.0f, 1.0f, 1.0f),
+                                        img.data(), cw, ch))
+        return 0;
+    for (int yy = 0; yy < hh; ++yy)
+        for (int xx = 0; xx < w; ++xx) out[yy * w + xx] = img[((size_t)yy * cw + xx) * 3];
+    return 1;
 }

@@ -51,6 +51,9 @@ class RefHelloMonkey:
                 "mkrh_rotate_cpr": [vp, C.c_float, C.c_int], "mkrh_reset": [vp],
                 "mkrh_set_tf": [vp, vp, vp, C.c_int, vp, vp, C.c_int, C.c_int],
                 "mkrh_vr_image": [vp, vp, C.c_longlong, vp], "mkrh_plane_image": [vp, C.c_int, vp, C.c_longlong, vp],
+                "mkrh_add_annotation": [vp, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float,
+                                        C.c_float, C.c_float],
+                "mkrh_remove_annotations": [vp],
             }
             for f, a in sig.items():
                 getattr(L, f).argtypes = a
@@ -147,6 +150,13 @@ def run_both(p, ops, masks=None):
             L.mkrh_set_cpr_line_voxel(h, ptr(pts), len(pts)); mine.SetCPRLineVoxelArray(pts)
         elif k == "rotate_cpr":
             L.mkrh_rotate_cpr(h, op[1], op[2]); mine.RotateCPR(op[1], pm.PlaneType(op[2]))
+        elif k == "annotation":
+            txt, x, y, fs, fmt, rgba = op[1:]
+            L.mkrh_add_annotation(h, txt.encode(), x, y, fs, fmt, *rgba)
+            mine.AddAnnotation(pm.PlaneType.PlaneVR, txt, x, y, pm.FontSize(fs), pm.AnnotationFormat(fmt),
+                               pm.RGBA(*rgba))
+        elif k == "clear_annotations":
+            L.mkrh_remove_annotations(h); mine.RemoveAllAnnotations()
         else:
             raise ValueError(k)
     return ref, mine
@@ -264,3 +274,29 @@ def test_png_strings_decode_to_the_images(phantom):
     raw = zlib.decompress(png[i + 4:i + 4 + n])
     img = np.frombuffer(raw, np.uint8).reshape(h, 1 + w * 3)[:, 1:].reshape(h, w, 3)
     assert np.array_equal(img, mine.GetVRImage())
+
+
+def test_text_annotations_in_vr(phantom):
+    """VR images with MonkeyGL's annotation layer: text of the three font
+    sizes and alignments, clipped at the image edges, drawn after the
+    orientation box (core/VRProvider.cpp:30-36, core/AnnotationLayer.cpp:41-61).
+    Both objects load their glyphs and mesh from oracle/_ref/resources."""
+    anns = [("annotation", "MonkeyGL B200 - VR 512x512", 6, 4, 0, 0, (1.0, 1.0, 0.0, 1.0)),
+            ("annotation", "WW/WL: 1700/650", 506, 30, 1, 1, (0.2, 0.9, 1.0, 1.0)),
+            ("annotation", "Axial {R} [x] ~`!@#$%^&*()", 256, 240, 2, 2, (1.0, 0.5, 0.25, 1.0)),
+            ("annotation", "edge clip", 480, 500, 2, 0, (0.9, 0.9, 0.9, 1.0)),
+            ("annotation", "left clip", -30, -10, 1, 0, (0.5, 1.0, 0.5, 1.0))]
+    ops = [("clear_annotations",), ("tf", TF4, {}, -1), ("wwwl", 1700, 650, -1), ("rotate", 25, 5)] + anns
+    try:
+        ref, mine = run_both(phantom, ops)
+        img = mine.GetVRImage()
+        assert_vr_equal(img, ref_vr(ref), "VR with text annotations")
+        # the text is there: the same view without annotations differs
+        L, h = ref.L, ref.h
+        L.mkrh_remove_annotations(h)
+        mine.RemoveAllAnnotations()
+        plain = mine.GetVRImage()
+        assert_vr_equal(plain, ref_vr(ref), "VR after removing the annotations")
+        assert int(np.count_nonzero((img != plain).any(-1))) > 500
+    finally:
+        RefHelloMonkey().L.mkrh_remove_annotations(RefHelloMonkey().h)

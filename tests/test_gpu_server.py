@@ -200,3 +200,33 @@ def test_eviction_under_a_budget_below_the_volumes(vols):
         with pytest.raises(capi.MonkeyGLError) as e:
             srv.add_volume(big.volume)
         assert e.value.status == capi.MK_ERR_BUDGET
+
+
+def test_encoded_output_decodes_to_the_image(vols):
+    """Requests that ask for MonkeyGL's *_pngString form (a Base64 PNG; a
+    plane as W/2 RGBA pixels) get it written by the server's encoder thread:
+    alone and mixed, it decodes to the request's own image, which equals the
+    plain path's."""
+    import sys
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent))
+    from pngcheck import decode_png_base64
+    reqs = serving_trace(specs(vols), 24, 1000.0, seed=13, sizes=(64, 96, 128))
+    plain = plain_images(vols, reqs)
+    with srvmod.Server(max_slots=4, max_pending=64, max_pixels=128 * 128, max_labels=8, tiles_per_step=40) as srv:
+        vids = [srv.add_volume(p.volume, p.labels) for p in vols]
+        for rnd in range(2):
+            if rnd == 0:
+                got = [srv.wait(srvmod.submit_request(srv, vids[r.volume], r, encode=True)) for r in reqs]
+            else:
+                tickets = [srvmod.submit_request(srv, vids[r.volume], r, encode=(i % 2 == 0))
+                           for i, r in enumerate(reqs)]
+                got = [srv.wait(t) for t in tickets]
+            for i, ((img, tm), r) in enumerate(zip(got, reqs)):
+                assert np.array_equal(img, plain[i]), f"round {rnd} request {i}"
+                if "png_base64" not in tm:
+                    assert rnd == 1 and i % 2 == 1
+                    continue
+                dec = decode_png_base64(tm["png_base64"])
+                if r.kind == capi.REQUEST_MPR:
+                    dec = dec.reshape(r.size, -1).view(np.int16)
+                assert np.array_equal(dec, img), f"round {rnd} request {i}: the encoded form differs"

@@ -100,3 +100,64 @@ def test_invalid_arguments():
     assert capi.lib().mk_mesh_load_stl(b"/nonexistent/human.stl", C.byref(h)) == capi.MK_ERR_INVALID_ARGUMENT
     assert capi.lib().mk_merge_orientation_box(None, None, None, 512, 512) == capi.MK_ERR_INVALID_ARGUMENT
     assert capi.lib().mk_draw_line_rgb(None, 10, 10, 0, 0, 1, 1, 1, None) == capi.MK_ERR_INVALID_ARGUMENT
+
+
+GLYPHS = ROOT / "oracle" / "_ref" / "resources" / "annotation_glyphs.bin"
+REF_HOST = ROOT / "oracle" / "_ref" / "libmkref_host.so"
+
+
+@pytest.fixture(scope="module")
+def font():
+    if not GLYPHS.exists() or not REF_HOST.exists():
+        pytest.skip("MonkeyGL's glyphs not extracted: run `make -C oracle ref` with the MonkeyGL sources")
+    h = C.c_void_p()
+    assert capi.lib().mk_font_load(str(GLYPHS).encode(), C.byref(h)) == capi.MK_OK, capi.lib().mk_last_error()
+    yield h
+    capi.lib().mk_font_destroy(h)
+
+
+def test_text_matches_monkeygl_textout(font):
+    """mk_draw_text_rgb against MonkeyGL's AnnotationUtils::Textout2Image
+    (its host library, built from its sources): random printable strings
+    with a few bytes that have no glyph, every font size (and an undefined
+    one), the three alignments, positions that clip at every edge, random
+    colours, several image sizes; plus mk_text_size against GetSize."""
+    L = C.CDLL(str(REF_HOST))
+    L.mkrh_textout.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                               C.c_void_p, C.c_int, C.c_int]
+    rng = np.random.default_rng(77)
+    printable = [bytes([c]) for c in range(0x20, 0x7f)]
+    extra = ["·".encode(), "é".encode(), b"\t"]
+    n = 0
+    for case in range(400):
+        k = int(rng.integers(0, 14))
+        text = b"".join(printable[int(i)] for i in rng.integers(0, len(printable), k))
+        if case % 7 == 0:
+            text += extra[case % 3] + b"Z"
+        w, h = [(512, 512), (97, 41), (10, 10), (300, 64)][case % 4]
+        x = int(rng.integers(-60, w + 20))
+        y = int(rng.integers(-50, h + 10))
+        size = int(rng.integers(-1, 3))
+        fmt = int(rng.integers(0, 3))
+        col = rng.uniform(0, 1, 3).astype(np.float32)
+        if case % 11 == 0:
+            col = np.array([1.0, 1.0, 1.0], np.float32)
+        mine = rng.integers(0, 256, (h, w, 3), dtype=np.uint8)
+        ref = mine.copy()
+        rc = capi.lib().mk_draw_text_rgb(font, _ptr(mine), w, h, text, x, y, size, fmt, _ptr(col))
+        ok = L.mkrh_textout(text, x, y, size, fmt, float(col[0]), float(col[1]), float(col[2]), _ptr(ref), w, h)
+        assert (rc == capi.MK_OK) == (ok == 1)
+        diff = int(np.count_nonzero(mine != ref))
+        assert diff == 0, f"case {case}: text {text!r} at ({x}, {y}) size {size} format {fmt}: {diff} values differ"
+        n += int(np.count_nonzero(mine))
+    assert n > 0
+    # refused like MonkeyGL: images below 10 pixels, an undefined format
+    img = np.zeros((9, 40, 3), np.uint8)
+    col = np.ones(3, np.float32)
+    assert capi.lib().mk_draw_text_rgb(font, _ptr(img), 40, 9, b"A", 0, 0, 0, 0, _ptr(col)) != capi.MK_OK
+    assert capi.lib().mk_draw_text_rgb(font, _ptr(img), 40, 9, b"A", 0, 0, 0, -1, _ptr(col)) != capi.MK_OK
+    w, h = C.c_int(), C.c_int()
+    assert capi.lib().mk_text_size(font, b"Hello, 3D", 1, C.byref(w), C.byref(h)) == capi.MK_OK
+    assert w.value > 0 and h.value == 33
+    assert capi.lib().mk_text_size(font, b"a\xc2\xb7", 0, C.byref(w), C.byref(h)) == capi.MK_OK
+    assert h.value == -1
