@@ -18,14 +18,17 @@
 // Backward.  With g = dL/dC and U_i the colour composited behind sample i
 // seen from unit transmittance just after it (U_last = 0,
 // U_{i-1} = a_i c_i + (1 - a_i) U_i),
-//     dL/dc_i = T_i a_i g,     dL/da_i = T_i g . (c_i - U_i),
-// with no division by (1 - a_i).  T_i comes from per-ray checkpoints of T
-// every K samples: the backward walks segments of 16 samples from last to
-// first, re-marching each forward from its checkpoint and keeping the sample
-// values and transmittances in registers.  A ray accumulates its dL/dLUT in
-// registers while its samples stay in one LUT cell and its dL/dvolume while
-// they stay in one voxel cell; a change of cell flushes the sums (shared-
-// memory bins for the LUT, eight global reductions for the voxels).
+//     dL/dc_i = T_i a_i g,     dL/da_i = T_i g . (c_i - U_i).
+// The backward reverse-marches each ray from its last sample, reconstructing
+// T_i = T_{i+1} / (1 - a_i) from the transmittance the forward saved after
+// the last sample; the forward also saves T every K samples (checkpoints),
+// which reset the reconstruction at each checkpoint and give T_i where
+// a_i = 1 leaves nothing to divide by (a re-march from the checkpoint).  A
+// ray accumulates its dL/dLUT in registers while its samples stay in one LUT
+// cell and its dL/dvolume while they stay in one voxel cell; a change of
+// cell flushes the sums -- the LUT sums of the lanes flushing one cell are
+// combined by warp shuffles before the shared-memory bins, which go to global
+// memory once per block; the voxel sums take eight global reductions.
 #include <cuda_runtime.h>
 #include <limits.h>
 #include <math.h>
@@ -253,23 +256,61 @@ __global__ void __launch_bounds__(256) k_dvr_forward(const __grid_constant__ Dvr
     images[3 * o + 1] = cg;
     images[3 * o + 2] = cb;
     trans[o] = T;
-    if (wk) reinterpret_cast<int *>(wk + (size_t)V.max_ckpt * npix)[pix] = i;   // samples taken
+    if (wk) {
+        reinterpret_cast<int *>(wk + (size_t)V.max_ckpt * npix)[pix] = i;   // samples taken
+        wk[(size_t)(V.max_ckpt + 1) * npix + pix] = T;                      // transmittance after them
+    }
 }
 
 // ---------------------------------------------------------------------------
 // backward: 128 threads = 16x8 pixels as 8x4 warp tiles; blockIdx.z = view
 
-__device__ __forceinline__ void flush_lut(float *bins, int n, int k, const float4 &a0, const float4 &a1) {
-    if (k < 0) return;
-    atomicAdd(&bins[4 * k + 0], a0.x);
-    atomicAdd(&bins[4 * k + 1], a0.y);
-    atomicAdd(&bins[4 * k + 2], a0.z);
-    atomicAdd(&bins[4 * k + 3], a0.w);
-    if (k + 1 < n) {
-        atomicAdd(&bins[4 * k + 4], a1.x);
-        atomicAdd(&bins[4 * k + 5], a1.y);
-        atomicAdd(&bins[4 * k + 6], a1.z);
-        atomicAdd(&bins[4 * k + 7], a1.w);
+// Adds the LUT-gradient runs that lanes end at this step (cell k: a0 to
+// entry k, a1 to entry k + 1) to the block's shared bins.  Every lane of the
+// warp calls it.  Lanes ending a run on the same cell are summed by warp
+// shuffles first (a butterfly per cell), so a cell takes one set of
+// shared-memory atomics per warp and step; a lane alone on its cell adds
+// directly.
+__device__ __forceinline__ void flush_lut_warp(float *bins, int n, bool flush, int k, const float4 &a0,
+                                               const float4 &a1) {
+    const unsigned FULL = 0xffffffffu;
+    if (__ballot_sync(FULL, flush) == 0u) return;
+    const int lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(FULL, flush ? k : -1);
+    const bool alone = flush && __popc(peers) == 1;
+    if (alone) {
+        atomicAdd(&bins[4 * k + 0], a0.x);
+        atomicAdd(&bins[4 * k + 1], a0.y);
+        atomicAdd(&bins[4 * k + 2], a0.z);
+        atomicAdd(&bins[4 * k + 3], a0.w);
+        if (k + 1 < n) {
+            atomicAdd(&bins[4 * k + 4], a1.x);
+            atomicAdd(&bins[4 * k + 5], a1.y);
+            atomicAdd(&bins[4 * k + 6], a1.z);
+            atomicAdd(&bins[4 * k + 7], a1.w);
+        }
+    }
+    unsigned shared = __ballot_sync(FULL, flush && !alone);
+    while (shared) {
+        const int leader = __ffs(shared) - 1;
+        const unsigned grp = __shfl_sync(FULL, peers, leader);
+        const bool in = (grp >> lane) & 1u;
+        float v[8] = {in ? a0.x : 0.f, in ? a0.y : 0.f, in ? a0.z : 0.f, in ? a0.w : 0.f,
+                      in ? a1.x : 0.f, in ? a1.y : 0.f, in ? a1.z : 0.f, in ? a1.w : 0.f};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) v[c] += __shfl_xor_sync(FULL, v[c], o);
+        }
+        if (lane == leader) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) atomicAdd(&bins[4 * k + c], v[c]);
+            if (k + 1 < n) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) atomicAdd(&bins[4 * k + 4 + c], v[4 + c]);
+            }
+        }
+        shared &= ~grp;
     }
 }
 
@@ -286,6 +327,15 @@ __device__ __forceinline__ void flush_vol(float *__restrict__ gv, const DvrBatch
     }
 }
 
+// Reverse march.  A ray walks its samples from the last to the first,
+// reconstructing T_i = T_{i+1} / (1 - a_i) from the transmittance saved after
+// its last sample; at every checkpoint (each 2^ckpt_shift samples) T is taken
+// from the forward pass instead, so a reconstruction never runs for more
+// than one checkpoint interval.  A sample with a_i = 1 (nothing to divide
+// by) takes T_i by re-marching forward from its interval's checkpoint.  Each
+// sample is fetched once otherwise.  The walk is warp-uniform (lanes past
+// their first sample idle), so the LUT-gradient runs that end in one step
+// can be combined across the warp.
 template <bool VOLGRAD>
 __global__ void __launch_bounds__(128) k_dvr_backward(const __grid_constant__ DvrBatch B,
                                                       const float *__restrict__ vol,
@@ -303,96 +353,111 @@ __global__ void __launch_bounds__(128) k_dvr_backward(const __grid_constant__ Dv
 
     const DvrView &V = B.v[blockIdx.z];
     const int x = pixel_x(blockIdx.x, 16), y = pixel_y(blockIdx.y, 16);
-    if (x < B.W && y < B.H) {
-        const size_t npix = (size_t)B.W * B.H, pix = (size_t)y * B.W + x;
-        const float *wk = work + V.work_off;
-        const size_t o = (size_t)blockIdx.z * npix + pix;
-        const float gr = grad_images[3 * o], gg = grad_images[3 * o + 1], gb = grad_images[3 * o + 2];
-        int ns = reinterpret_cast<const int *>(wk + (size_t)V.max_ckpt * npix)[pix];
+    const bool in_image = x < B.W && y < B.H;
+    const size_t npix = (size_t)B.W * B.H, pix = in_image ? (size_t)y * B.W + x : 0;
+    const float *wk = work + V.work_off;
+    const size_t o = (size_t)blockIdx.z * npix + pix;
+    float gr = 0.f, gg = 0.f, gb = 0.f, T = 0.f;
+    int ns = 0;
+    if (in_image) {
+        gr = grad_images[3 * o];
+        gg = grad_images[3 * o + 1];
+        gb = grad_images[3 * o + 2];
+        ns = reinterpret_cast<const int *>(wk + (size_t)V.max_ckpt * npix)[pix];
+        T = wk[(size_t)(V.max_ckpt + 1) * npix + pix];
         if (gr == 0.0f && gg == 0.0f && gb == 0.0f) ns = 0;
-        const Ray r = make_ray(B, V, x, y);
-        float Ur = 0.f, Ug = 0.f, Ub = 0.f;
-        int lk = -1;
-        float4 la0 = make_float4(0.f, 0.f, 0.f, 0.f), la1 = la0;
-        int vx = INT_MIN, vy = 0, vz = 0;
-        float va[8];
+    }
+    const Ray r = make_ray(B, V, x, y);
+    const int cmask = (1 << V.ckpt_shift) - 1;
+    int steps = ns;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) va[c] = 0.0f;
+    for (int off = 16; off > 0; off >>= 1) steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, off));
+    float Ur = 0.f, Ug = 0.f, Ub = 0.f;
+    int lk = -1;
+    float4 la0 = make_float4(0.f, 0.f, 0.f, 0.f), la1 = la0;
+    int vx = INT_MIN, vy = 0, vz = 0;
+    float va[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) va[c] = 0.0f;
 
-        for (int seg = (ns + kDvrSeg - 1) / kDvrSeg - 1; seg >= 0; --seg) {
-            const int s0 = seg * kDvrSeg;
-            const int c0 = s0 >> V.ckpt_shift;
-            float T = wk[(size_t)c0 * npix + pix];
-            for (int i = c0 << V.ckpt_shift; i < s0; ++i)
-                T *= 1.0f - lut_value(L, D, lut_cell(trilinear(B, vol, sample_cell(B, r, V.step, i)), n)).w;
-            const int s1 = min(s0 + kDvrSeg, ns) - s0;
-            float Ts[kDvrSeg], Ss[kDvrSeg];
-#pragma unroll
-            for (int j = 0; j < kDvrSeg; ++j) {
-                Ts[j] = T;
-                Ss[j] = 0.0f;
-                if (j < s1) {
-                    const float s = trilinear(B, vol, sample_cell(B, r, V.step, s0 + j));
-                    Ss[j] = s;
-                    T *= 1.0f - lut_value(L, D, lut_cell(s, n)).w;
-                }
+    for (int t = 0; t < steps; ++t) {
+        const int i = ns - 1 - t;
+        const bool live = i >= 0;
+        LutCell h;
+        h.k = -1;
+        h.w = 0.0f;
+        h.inside = false;
+        float d_cr = 0.f, d_cg = 0.f, d_cb = 0.f, d_a = 0.f;
+        Cell c = {};
+        if (live) {
+            c = sample_cell(B, r, V.step, i);
+            h = lut_cell(trilinear(B, vol, c), n);
+            const float4 q = lut_value(L, D, h);
+            const float d = 1.0f - q.w;
+            float Ti;
+            if ((i & cmask) == 0) {
+                Ti = wk[(size_t)(i >> V.ckpt_shift) * npix + pix];
+            } else if (d != 0.0f) {
+                Ti = T / d;
+            } else {
+                Ti = wk[(size_t)(i >> V.ckpt_shift) * npix + pix];
+                for (int j = i & ~cmask; j < i; ++j)
+                    Ti *= 1.0f - lut_value(L, D, lut_cell(trilinear(B, vol, sample_cell(B, r, V.step, j)), n)).w;
             }
+            T = Ti;
+            d_cr = Ti * q.w * gr;
+            d_cg = Ti * q.w * gg;
+            d_cb = Ti * q.w * gb;
+            d_a = Ti * (gr * (q.x - Ur) + gg * (q.y - Ug) + gb * (q.z - Ub));
+            Ur = q.w * q.x + (1.0f - q.w) * Ur;
+            Ug = q.w * q.y + (1.0f - q.w) * Ug;
+            Ub = q.w * q.z + (1.0f - q.w) * Ub;
+        }
+        const bool change = live && h.k != lk;
+        flush_lut_warp(bins, n, change && lk >= 0, lk, la0, la1);
+        if (change) {
+            lk = h.k;
+            la0 = make_float4(0.f, 0.f, 0.f, 0.f);
+            la1 = la0;
+        }
+        if (live) {
+            const float w1 = h.w, w0 = 1.0f - h.w;
+            la0.x += w0 * d_cr;
+            la0.y += w0 * d_cg;
+            la0.z += w0 * d_cb;
+            la0.w += w0 * d_a;
+            la1.x += w1 * d_cr;
+            la1.y += w1 * d_cg;
+            la1.z += w1 * d_cb;
+            la1.w += w1 * d_a;
+            if (VOLGRAD && h.inside) {
+                const float4 dd = D[h.k];
+                const float ds = (float)n * (d_cr * dd.x + d_cg * dd.y + d_cb * dd.z + d_a * dd.w);
+                if (ds != 0.0f) {
+                    if (c.ix != vx || c.iy != vy || c.iz != vz) {
+                        flush_vol(grad_vol, B, vx, vy, vz, va);
+                        vx = c.ix;
+                        vy = c.iy;
+                        vz = c.iz;
 #pragma unroll
-            for (int j = kDvrSeg - 1; j >= 0; --j) {
-                if (j >= s1) continue;
-                const LutCell h = lut_cell(Ss[j], n);
-                const float4 q = lut_value(L, D, h);
-                const float Ti = Ts[j];
-                const float d_cr = Ti * q.w * gr, d_cg = Ti * q.w * gg, d_cb = Ti * q.w * gb;
-                const float d_a = Ti * (gr * (q.x - Ur) + gg * (q.y - Ug) + gb * (q.z - Ub));
-                Ur = q.w * q.x + (1.0f - q.w) * Ur;
-                Ug = q.w * q.y + (1.0f - q.w) * Ug;
-                Ub = q.w * q.z + (1.0f - q.w) * Ub;
-                if (h.k != lk) {
-                    flush_lut(bins, n, lk, la0, la1);
-                    lk = h.k;
-                    la0 = make_float4(0.f, 0.f, 0.f, 0.f);
-                    la1 = la0;
-                }
-                const float w1 = h.w, w0 = 1.0f - h.w;
-                la0.x += w0 * d_cr;
-                la0.y += w0 * d_cg;
-                la0.z += w0 * d_cb;
-                la0.w += w0 * d_a;
-                la1.x += w1 * d_cr;
-                la1.y += w1 * d_cg;
-                la1.z += w1 * d_cb;
-                la1.w += w1 * d_a;
-                if (VOLGRAD && h.inside) {
-                    const float4 d = D[h.k];
-                    const float ds = (float)n * (d_cr * d.x + d_cg * d.y + d_cb * d.z + d_a * d.w);
-                    if (ds != 0.0f) {
-                        const Cell c = sample_cell(B, r, V.step, s0 + j);
-                        if (c.ix != vx || c.iy != vy || c.iz != vz) {
-                            flush_vol(grad_vol, B, vx, vy, vz, va);
-                            vx = c.ix;
-                            vy = c.iy;
-                            vz = c.iz;
-#pragma unroll
-                            for (int k = 0; k < 8; ++k) va[k] = 0.0f;
-                        }
-                        const float y0z0 = (1.0f - c.wy) * (1.0f - c.wz) * ds, y1z0 = c.wy * (1.0f - c.wz) * ds;
-                        const float y0z1 = (1.0f - c.wy) * c.wz * ds, y1z1 = c.wy * c.wz * ds;
-                        va[0] += (1.0f - c.wx) * y0z0;
-                        va[1] += c.wx * y0z0;
-                        va[2] += (1.0f - c.wx) * y1z0;
-                        va[3] += c.wx * y1z0;
-                        va[4] += (1.0f - c.wx) * y0z1;
-                        va[5] += c.wx * y0z1;
-                        va[6] += (1.0f - c.wx) * y1z1;
-                        va[7] += c.wx * y1z1;
+                        for (int k = 0; k < 8; ++k) va[k] = 0.0f;
                     }
+                    const float y0z0 = (1.0f - c.wy) * (1.0f - c.wz) * ds, y1z0 = c.wy * (1.0f - c.wz) * ds;
+                    const float y0z1 = (1.0f - c.wy) * c.wz * ds, y1z1 = c.wy * c.wz * ds;
+                    va[0] += (1.0f - c.wx) * y0z0;
+                    va[1] += c.wx * y0z0;
+                    va[2] += (1.0f - c.wx) * y1z0;
+                    va[3] += c.wx * y1z0;
+                    va[4] += (1.0f - c.wx) * y0z1;
+                    va[5] += c.wx * y0z1;
+                    va[6] += (1.0f - c.wx) * y1z1;
+                    va[7] += c.wx * y1z1;
                 }
             }
         }
-        flush_lut(bins, n, lk, la0, la1);
-        if (VOLGRAD) flush_vol(grad_vol, B, vx, vy, vz, va);
     }
+    flush_lut_warp(bins, n, lk >= 0, lk, la0, la1);
+    if (VOLGRAD) flush_vol(grad_vol, B, vx, vy, vz, va);
     __syncthreads();
     for (int i = threadIdx.x; i < 4 * n; i += blockDim.x) {
         const float v = bins[i];
@@ -413,11 +478,12 @@ static void view_layout(const mk_dvr_params &p, int &ckpt_shift, int &max_ckpt) 
     max_ckpt = (steps + (1 << sh) - 1) >> sh;
 }
 
-// Workspace floats of one view: max_ckpt checkpoint planes + one plane of counts.
+// Workspace floats of one view: max_ckpt checkpoint planes, a plane of sample
+// counts and a plane of final transmittances.
 static size_t view_floats(const mk_dvr_params &p) {
     int sh, mc;
     view_layout(p, sh, mc);
-    return (size_t)(mc + 1) * p.width * p.height;
+    return (size_t)(mc + 2) * p.width * p.height;
 }
 
 static int check_views(const mk_dvr_params *views, int nviews) {

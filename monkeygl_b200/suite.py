@@ -6,8 +6,10 @@ Rows (synthetic seeded phantoms of monkeygl_b200.phantom):
     background opacity caps 0.4 and 0.8;
   * MPR of the cardiac phantom: axial, sagittal, coronal and 8 seeded oblique
     planes of 512^2, trilinear and nearest, slab of 1 sample;
-  * CPR of a cardiac vessel, 1024 rows x 512 columns, stretched and
-    straightened;
+  * CPR of a body vessel (200-point Catmull-Rom centreline), 1024 rows x 512
+    columns, stretched and straightened;
+  * VR of the body phantom with a dense transfer function (soft tissue
+    visible), where empty-space skipping cannot help inside the body;
   * differentiable VR: float32 256^3 volume, 256-entry LUT, 8 views of 256^2,
     step 0.5 voxel -- forward, backward and their ratio;
   * GetVRData through the HelloMonkey API (render, orientation box, copy
@@ -71,11 +73,26 @@ def _workload(ctx, name, bg=0.4):
     return make_workload(name, bg_alpha=bg, phantom=ph[name])
 
 
-def vr_rows(name, bg, rtypes, ctx):
+def dense_luts(w):
+    """A transfer function with soft tissue visible: alpha rises from 0 at
+    -200 HU to 0.03 at about 0 HU (the body's 40 +- 20 HU), 0.12 at 300 HU
+    and 0.9 at 1500 HU, so rays composite (and refine their step) all
+    through the body and empty-space skipping cannot help inside it.  Same
+    colours for every label."""
+    from monkeygl_b200.phantom import make_tf_lut
+    pts = [(0.0, (0.8, 0.5, 0.4, 0.0)), (0.12, (0.85, 0.55, 0.45, 0.03)), (0.3, (0.9, 0.7, 0.6, 0.12)),
+           (1.0, (1.0, 0.95, 0.9, 0.9))]
+    lut = make_tf_lut(pts)
+    return {l: lut for l in w.luts}
+
+
+def vr_rows(name, bg, rtypes, ctx, dense=False):
     import torch
     from monkeygl_b200 import capi
     from monkeygl_b200.workloads import view_camera
     w = _workload(ctx, name, bg)
+    if dense:
+        w.luts = dense_luts(w)
     vol = capi.Volume(w.phantom.volume)
     if w.phantom.labels is not None:
         vol.set_mask(w.phantom.labels)
@@ -98,7 +115,8 @@ def vr_rows(name, bg, rtypes, ctx):
         ms = _median_ms(lambda i: vol.render_vr_device(params[i % n], out.data_ptr(), stream.cuda_stream),
                         n, stream, ctx["flush"])
         e2e = _wall_ms(lambda i: vol.render_vr(params[i % n], out=host), n)
-        row = {"row": f"{'VR' if rt == 0 else 'MIP'} {name}" + (f" bg {bg}" if name == "body" else ""),
+        row = {"row": f"{'VR' if rt == 0 else 'MIP'} {name}" + (f" bg {bg}" if name == "body" else "") +
+                      (" dense TF (soft tissue visible)" if dense else ""),
                "image": f"{size}x{size}", "views": n, "ms": round(ms, 4), "fps": round(1e3 / ms, 1),
                "e2e_ms": round(e2e, 4)}
         if ref is not None:
@@ -150,9 +168,9 @@ def cpr_rows(ctx):
     import torch
     from monkeygl_b200 import capi
     from monkeygl_b200.workloads import cpr_straightened, cpr_stretched, vessel_path
-    w = _workload(ctx, "cardiac")
+    w = _workload(ctx, "body")
     vol = capi.Volume(w.phantom.volume)
-    path = vessel_path(w.phantom, rows=1024)
+    path = vessel_path(w.phantom, n_points=200, rows=1024)
     width = 512
     out = torch.empty(1024 * width, dtype=torch.int16, device="cuda")
     ref = ctx["ref"]
@@ -176,7 +194,7 @@ def cpr_rows(ctx):
             dev(i)
         ms = _median_ms(dev, 20, stream, ctx["flush"])
         e2e = _wall_ms(lambda i: vol.render_cpr(width, pts, dirs, False), 20)
-        row = {"row": f"CPR cardiac {builder.__name__.split('_')[1]}", "image": f"{width}x{h}", "ms": round(ms, 4),
+        row = {"row": f"CPR body {builder.__name__.split('_')[1]}", "image": f"{width}x{h}", "ms": round(ms, 4),
                "e2e_ms": round(e2e, 4)}
         if ref is not None:
             rms = _wall_ms(lambda i: ref.cpr(width, pts, dirs, False), 10)
@@ -232,8 +250,9 @@ def dvr_rows(ctx):
                                 C.c_void_p(imgs.data_ptr()), C.c_void_p(tr.data_ptr()), C.c_void_p(work.data_ptr()),
                                 None), "mk_dvr_forward")
     torch.cuda.synchronize()
-    per = work.numel() // 8
-    samples = sum(int(work[i * per + per - 256 * 256:(i + 1) * per].view(torch.int32).sum().item())
+    # per view: checkpoint planes, then a plane of sample counts, then one of final transmittances
+    per, npix = work.numel() // 8, 256 * 256
+    samples = sum(int(work[i * per + per - 2 * npix:i * per + per - npix].view(torch.int32).sum().item())
                   for i in range(8))
     f, b = statistics.median(fw), statistics.median(bw)
     return [{"row": "DVR 256^3, 8 views 256^2 (forward)", "ms": round(f, 4), "samples": samples,
@@ -325,6 +344,7 @@ def main(args=None, ref=None, ref_api=None, resources_dir=None):
         rows += vr_rows("cardiac", 0.4, (0, 1), ctx)
         rows += vr_rows("body", 0.4, (0,), ctx)
         rows += vr_rows("body", 0.8, (0,), ctx)
+        rows += vr_rows("body", 0.4, (0,), ctx, dense=True)
     if want("mpr"):
         rows += mpr_rows(ctx)
     if want("cpr"):

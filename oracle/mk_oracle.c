@@ -720,3 +720,117 @@ int mko_dvr_forward_d(const double *p, const double *vol, const double *lut, int
     (void)nthreads;
     return 0;
 }
+
+/* Conditioning of a reverse march for the differentiable method: per ray, the
+ * forward transmittances T_i in FP32, then T reconstructed backwards from the
+ * final T by T_i = T_{i+1} / (1 - a_i) (the division a checkpoint-free
+ * backward would make), compared with the forward values.  stats receives:
+ * [0] rays with samples, [1] rays whose reconstruction is off by more than
+ * 1e-3 relative at some sample (or divides by zero), [2] rays that meet an
+ * opaque sample (1 - a_i == 0 in FP32), [3] the largest relative error over
+ * the rays that stay finite, [4] samples in all rays.  Test infrastructure:
+ * it measures the method, it renders nothing. */
+int mko_dvr_reverse_stats(const double *p, const float *vol, const float *lut, int nthreads, double *stats) {
+    const int w = (int)p[0], h = (int)p[1];
+    const int dim[3] = {(int)p[2], (int)p[3], (int)p[4]};
+    const double *mls = p + 5, *M = p + 8;
+    const double scale = p[17], xT = p[18], yT = p[19], step = p[20], t_min = p[21];
+    const int n_lut = (int)p[22];
+    if (w <= 0 || h <= 0 || dim[0] <= 0 || dim[1] <= 0 || dim[2] <= 0 || n_lut < 2 || !(step > 0)) return 1;
+    long long rays = 0, bad = 0, opaque = 0, samples = 0;
+    double worst = 0.0;
+#ifdef _OPENMP
+    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(+ : rays, bad, opaque, samples) reduction(max : worst)
+#endif
+    for (int y = 0; y < h; ++y) {
+        float *Ts = (float *)malloc(sizeof(float) * 8192), *as = (float *)malloc(sizeof(float) * 8192);
+        for (int x = 0; x < w; ++x) {
+            const double u = (x - w / 2.0 - xT) / h, v = (y - h / 2.0 - yT) / h;
+            double base[3], dir[3], lo = 0.0, hi = 1.732;
+            int hit = 1;
+            for (int k = 0; k < 3; ++k) {
+                base[k] = (M[3 * k] * u + M[3 * k + 1] * (-0.866 * scale) + M[3 * k + 2] * v) * mls[k] + 0.5;
+                dir[k] = M[3 * k + 1] * scale * mls[k];
+                if (fabs(dir[k]) < 1e-12) {
+                    if (base[k] < 0.0 || base[k] > 1.0) hit = 0;
+                    continue;
+                }
+                double t0 = -base[k] / dir[k], t1 = (1.0 - base[k]) / dir[k];
+                if (t0 > t1) { double t = t0; t0 = t1; t1 = t; }
+                if (t0 > lo) lo = t0;
+                if (t1 < hi) hi = t1;
+            }
+            if (!hit || !(lo < hi)) continue;
+            const double a0 = ceil(lo / step) * step;
+            int n = (int)floor((hi - a0) / step) + 1;
+            if (n > 8190) n = 8190;
+            float T = 1.0f;
+            int m = 0;
+            for (int i = 0; i < n; ++i) {
+                const double a = a0 + i * step;
+                float c[3], fr[3];
+                int i0[3];
+                for (int k = 0; k < 3; ++k) {
+                    c[k] = (float)((base[k] + a * dir[k]) * dim[k] - 0.5);
+                    float f = floorf(c[k]);
+                    i0[k] = (int)f;
+                    fr[k] = c[k] - f;
+                }
+                float s = 0.0f;
+                for (int dz = 0; dz < 2; ++dz)
+                    for (int dy = 0; dy < 2; ++dy)
+                        for (int dx = 0; dx < 2; ++dx) {
+                            int ix = clampi(i0[0] + dx, 0, dim[0] - 1);
+                            int iy = clampi(i0[1] + dy, 0, dim[1] - 1);
+                            int iz = clampi(i0[2] + dz, 0, dim[2] - 1);
+                            float wt = (dx ? fr[0] : 1 - fr[0]) * (dy ? fr[1] : 1 - fr[1]) * (dz ? fr[2] : 1 - fr[2]);
+                            s += wt * vol[((size_t)iz * dim[1] + iy) * dim[0] + ix];
+                        }
+                float xx = s * n_lut - 0.5f, f = floorf(xx), wgt = xx - f;
+                int k = (int)f, k0, k1;
+                if (k < 0) { k0 = k1 = 0; wgt = 0; }
+                else if (k >= n_lut - 1) { k0 = k1 = n_lut - 1; wgt = 0; }
+                else { k0 = k; k1 = k + 1; }
+                const float al = lut[4 * k0 + 3] + wgt * (lut[4 * k1 + 3] - lut[4 * k0 + 3]);
+                Ts[m] = T;
+                as[m] = al;
+                ++m;
+                T *= 1.0f - al;
+                if (T < t_min) break;
+            }
+            if (m == 0) continue;
+            ++rays;
+            samples += m;
+            float Tr = T;
+            int is_opaque = 0;
+            double e = 0.0;
+            for (int i = m - 1; i >= 0; --i) {
+                const float d = 1.0f - as[i];
+                if (d == 0.0f) {
+                    is_opaque = 1;
+                    break;
+                }
+                Tr = Tr / d;
+                const double ref = Ts[i] > 1e-30f ? Ts[i] : 1e-30;
+                const double r = fabs((double)Tr - Ts[i]) / ref;
+                if (!(r <= 1e30)) { is_opaque = 1; break; }
+                if (r > e) e = r;
+            }
+            if (is_opaque) { ++opaque; ++bad; }
+            else {
+                if (e > 1e-3) ++bad;
+                if (e > worst) worst = e;
+            }
+        }
+        free(Ts);
+        free(as);
+    }
+    stats[0] = (double)rays;
+    stats[1] = (double)bad;
+    stats[2] = (double)opaque;
+    stats[3] = worst;
+    stats[4] = (double)samples;
+    (void)nthreads;
+    return 0;
+}

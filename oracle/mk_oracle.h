@@ -82,6 +82,8 @@ int mko_render_cpr(const mko_volume *v, int w, int h, const double *pts, const d
  * [20] step, [21] t_min, [22] lut_len; vol and lut are doubles; image is
  * width*height*3 doubles. */
 int mko_dvr_forward_d(const double *p, const double *vol, const double *lut, int nthreads, double *image);
+/* Conditioning of a reverse march from the final transmittance (FP32); see mk_oracle.c. */
+int mko_dvr_reverse_stats(const double *p, const float *vol, const float *lut, int nthreads, double *stats);
 
 /* Single texture fetches, exposed for known-answer tests. */
 float mko_tex3d_linear(const mko_volume *v, float x, float y, float z);

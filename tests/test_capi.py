@@ -99,8 +99,9 @@ def test_dvr_host_validation():
     from monkeygl_b200.camera import view_camera
     a = dvr.dvr_params(64, 48, view_camera(0.0), (32, 32, 32), (1, 1, 1), 0.5, 0.0, 256)
     b = dvr.dvr_params(64, 48, view_camera(30.0), (32, 32, 32), (1, 1, 1), 0.25, 0.0, 256)
-    # checkpoint planes (16 samples apart, 1.74/step + 2 samples) + one plane of counts
-    per = lambda p: (((int(1.74 / p.step) + 2 + 15) // 16) + 1) * 64 * 48
+    # checkpoint planes (16 samples apart, 1.74/step + 2 samples), a plane of counts and one of
+    # final transmittances
+    per = lambda p: (((int(1.74 / p.step) + 2 + 15) // 16) + 2) * 64 * 48
     assert dvr.workspace_floats([a]) == per(a)
     assert dvr.workspace_floats([a, b]) == per(a) + per(b)
     L = dvr._lib()

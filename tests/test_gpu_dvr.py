@@ -212,7 +212,9 @@ def test_gradients_match_torch_autograd(setup, angle, t_min):
                             C.c_void_p(work.data_ptr()), None) == 0
     torch.cuda.synchronize()
     assert torch.equal(img2, img)
-    counts = work[-64 * 64:].view(torch.int32).view(64, 64)
+    # workspace: checkpoint planes, a plane of sample counts, a plane of final transmittances
+    counts = work[-2 * 64 * 64:-64 * 64].view(torch.int32).view(64, 64)
+    assert torch.equal(work[-64 * 64:].view(64, 64), tr)
     if t_min > 0:
         assert (tr < t_min).any() and (counts < counts.max()).any()    # some rays stopped early
     v2 = torch.tensor(vol, device="cuda", requires_grad=True)
