@@ -416,8 +416,8 @@ __device__ __forceinline__ bool tail_reached(const RayParams &P) {
 
 // Write ray R (opacity accumulators at s_acc[.][acc_tid]) to the spill list;
 // false when the list is full (the ray then keeps marching).
-template <int TRACK>
-__device__ __forceinline__ bool spill_ray(const RayParams &P, const VrRay &R, const float (*s_acc)[256],
+template <int TRACK, int NT>
+__device__ __forceinline__ bool spill_ray(const RayParams &P, const VrRay &R, const float (*s_acc)[NT],
                                           int acc_tid) {
     const unsigned i = atomicAdd(&P.tail[1], 1u);
     if (i >= (unsigned)P.spill_cap) return false;
@@ -439,8 +439,8 @@ __device__ __forceinline__ bool spill_ray(const RayParams &P, const VrRay &R, co
     return true;
 }
 
-template <int TRACK>
-__device__ __forceinline__ bool vr_cap_ok(const LabelSmem &S, const float (*s_acc)[256], const float *accLocal,
+template <int TRACK, int NT>
+__device__ __forceinline__ bool vr_cap_ok(const LabelSmem &S, const float (*s_acc)[NT], const float *accLocal,
                                           int label, int owner) {
     const signed char sl = S.slot[label];
     if (TRACK == kTrackLocal) return (sl != -2) && accLocal[label] < S.alpha[label];
@@ -449,8 +449,8 @@ __device__ __forceinline__ bool vr_cap_ok(const LabelSmem &S, const float (*s_ac
     return s_acc[sl][owner] < S.alpha[label];
 }
 
-template <int TRACK>
-__device__ __forceinline__ void vr_cap_add(const LabelSmem &S, float (*s_acc)[256], float *accLocal, int label,
+template <int TRACK, int NT>
+__device__ __forceinline__ void vr_cap_add(const LabelSmem &S, float (*s_acc)[NT], float *accLocal, int label,
                                            int owner, float A, float alpha) {
     const signed char sl = S.slot[label];
     if (TRACK == kTrackLocal) accLocal[label] += (1.0f - A) * alpha;
@@ -462,9 +462,9 @@ __device__ __forceinline__ void vr_cap_add(const LabelSmem &S, float (*s_acc)[25
 // ray's final colour in R.sum.  Groups widen as rays finish: whenever the
 // unfinished rays fit into groups twice as large, their states move to new
 // groups, so a warp's last ray is marched by all 32 lanes.
-template <int TRACK, bool EARLY_TAPS = false>
+template <int TRACK, bool EARLY_TAPS = false, int NT = 256>
 __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
-                             const LabelSmem &S, const BrickView &BV, float (*s_acc)[256], CoopSample *ws,
+                             const LabelSmem &S, const BrickView &BV, float (*s_acc)[NT], CoopSample *ws,
                              unsigned act, VrRay &R, const StepVec &dv, float3 L, bool may_spill) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -510,20 +510,40 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
         bool reported = false;
         int round = 0;
         while (true) {
-            // 1. this lane's sample, j steps ahead
+            // A round on step L1/4 always stops at its first sample: MonkeyGL
+            // either refines there (to L1/8, from a - (L1/4 - L1/8)) or
+            // composites it and coarsens (to L1, from a + L1).  Such a round
+            // evaluates both continuations: lane 0 the sample itself, lanes
+            // 1..hA the refined run, lanes hA+1.. the coarsened run; the
+            // sample's test picks the run that is walked.
+            const bool two = G >= 8 && !Q.done && Q.step == L4 && Q.a > 0.0f;
+            const int hA = G / 2 - 1;
+            // 1. this lane's sample: j steps ahead, or its place in its run
             float4 clr = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             float alpha_j = 0.0f;
             int flags = 0, label = 0, nskip = 0;
-            float aj = Q.a;
+            float aj = Q.a, sj = Q.step;
+            int jj = j;
+            if (two && j > 0) {
+                if (j <= hA) {
+                    sj = L8;
+                    aj = Q.a - (L4 - L8);
+                    jj = j - 1;
+                } else {
+                    sj = L1;
+                    aj = Q.a + L1;
+                    jj = j - hA - 1;
+                }
+            }
             if (!Q.done) {
                 const int kj = Q.lat >= 0 ? min(Q.lat + j, P.accu_len - 1) : -1;
                 if (kj >= 0) {
                     aj = P.accu[kj];
                 } else {
-                    // j sequential additions, as the walk makes them
+                    // sequential additions, as the walk makes them
 #pragma unroll
                     for (int k = 0; k < 31; ++k)
-                        if (k < j) aj += Q.step;
+                        if (k < jj) aj += sj;
                 }
                 if (!(aj < P.limit) || aj > Q.a_stop) {
                     flags = kCoopEnd;
@@ -536,7 +556,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                         flags = kCoopOutside;
                     } else {
                         bool empty = false;
-                        if (P.skip && Q.step == L1) {
+                        if (P.skip && sj == L1) {
                             const int b = brick_index(P, BV, ix, iy, iz);
                             empty = !((BV.visible_bits[b >> 5] >> (b & 31)) & 1u);
                             if (empty) {
@@ -553,7 +573,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                             // something that composites: its shading taps are
                             // fetched with the value, not after the LUT (one
                             // texture round trip less, more registers)
-                            const bool early = EARLY_TAPS && Q.step != L1;
+                            const bool early = EARLY_TAPS && sj != L1;
                             GradTaps taps = {};
                             if (early) taps = fetch_taps(vol, pos, P);
                             temp = (temp - S.wl[label]) / S.ww[label] + 0.5f;
@@ -561,8 +581,8 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                             const cudaTextureObject_t tf = S.tf[label];
                             const float4 col = tf ? tex1D<float4>(tf, temp) : make_float4(0.f, 0.f, 0.f, 0.f);
                             float alpha = col.w;
-                            if (Q.step == L4) alpha = 1 - powf(1 - alpha, 0.25f);
-                            else if (Q.step == L8) alpha = 1 - powf(1 - alpha, 0.125f);
+                            if (sj == L4) alpha = 1 - powf(1 - alpha, 0.25f);
+                            else if (sj == L8) alpha = 1 - powf(1 - alpha, 0.125f);
                             alpha_j = alpha;
                             if (alpha > 0.0005f) {
                                 if (!early) taps = fetch_taps(vol, pos, P);
@@ -589,48 +609,58 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
             // from the stopping lane (the same float operations as the walk).
             // Other rounds take the sample-by-sample walk.
             const float alpha_up = __shfl_up_sync(FULL, alpha_j, 1);
-            const float pre_j = j == 0 ? Q.aPre : alpha_up;
+            const float alpha_0 = __shfl_sync(FULL, alpha_j, lane & ~(G - 1));   // the group's lane 0
+            float pre_j = j == 0 ? Q.aPre : alpha_up;
+            if (two && j == 1) pre_j = Q.aPre;           // a refinement keeps aPre
+            if (two && j == hA + 1) pre_j = alpha_0;     // after sample 0 was walked
             const bool busy = (pre_j > alpha_j ? pre_j : alpha_j) > 0.001f;  // (alpha > aPre ? alpha : aPre) > 0.001
             const bool pos_a = aj > 0.0f;
-            const bool refine_j = pos_a && busy && Q.step != L8;
-            const bool stop_j = !pos_a || Q.step == L4 || (Q.step == L1 ? busy : !busy);
-            // A sample in a skippable empty brick (coarse step, not fetched)
-            // counts as a fetched sample of alpha 0: where the walk reaches
-            // it after an alpha <= 0.001 it skips it with aPre = 0 and no
-            // step change, exactly what an alpha-0 sample gives; after a
-            // larger alpha the walk has already stopped at the sample before.
-            const bool plain_j = (flags & (kCoopEnd | kCoopOutside)) == 0 &&
-                                 (flags & (kCoopFetched | kCoopEmpty)) != 0;
+            const bool refine_j = pos_a && busy && sj != L8;
+            const bool stop_j = !pos_a || sj == L4 || (sj == L1 ? busy : !busy);
+            const bool plain_j = (flags & (kCoopEnd | kCoopOutside | kCoopFetched)) == kCoopFetched;
             const unsigned plain_m = __ballot_sync(FULL, plain_j);
             const unsigned stop_m = __ballot_sync(FULL, stop_j);
             const unsigned refine_m = __ballot_sync(FULL, refine_j);
             const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
-            const bool simple = member && !Q.done && ((plain_m >> (g * G)) & gbits) == gbits;
+            const unsigned gplain = (plain_m >> (g * G)) & gbits;
             const unsigned gstop = (stop_m >> (g * G)) & gbits;
-            const int s_at = gstop ? __ffs(gstop) - 1 : G;        // first stopping sample, G: none
-            const bool s_refine = s_at < G && ((refine_m >> (g * G + s_at)) & 1u);
+            const unsigned grefine = (refine_m >> (g * G)) & gbits;
+            // the lanes of the run walked this round, [r_lo, r_hi]; in a
+            // two-continuation round the coarsened run follows sample 0
+            // (lead0), the refined one replaces it
+            int r_lo = 0, r_hi = G - 1;
+            bool lead0 = false;
+            if (two) {
+                if (grefine & 1u) {
+                    r_lo = 1;
+                    r_hi = hA;
+                } else {
+                    r_lo = hA + 1;
+                    lead0 = true;
+                }
+            }
+            const int r_n = r_hi - r_lo + 1;
+            const unsigned rmask = (r_n == 32 ? 0xffffffffu : ((1u << r_n) - 1u)) << r_lo;
+            const unsigned need = rmask | (two ? 1u : 0u);
+            const bool simple = member && !Q.done && (gplain & need) == need;
+            const unsigned rstop = gstop & rmask;
+            const int s_at = rstop ? __ffs(rstop) - 1 : r_hi + 1;  // first stopping sample, r_hi + 1: none
+            const bool none = s_at > r_hi;
+            const bool s_refine = !none && ((grefine >> s_at) & 1u);
             {
-                // values of the stopping lane (or of the last lane when none stops)
-                const float ns = pos_a ? (Q.step == L8 ? L4 : L1) : Q.step;
+                // values of the stopping lane (or of the run's last lane when none stops)
+                const float ns = pos_a ? (sj == L8 ? L4 : L1) : sj;
                 float a_out, pre_out, step_out;
                 int lat_out;
-                if (s_at == G) {                    // all samples walked: a += step
-                    a_out = aj + Q.step;
+                if (none) {                         // all samples walked: a += step
+                    a_out = aj + sj;
                     pre_out = alpha_j;
-                    step_out = Q.step;
-                    lat_out = Q.lat >= 0 ? Q.lat + G : Q.lat;
-                    if ((flags & (kCoopEmpty | kCoopFetched)) == kCoopEmpty && nskip > 0) {
-                        // the last sample starts a skip: the walk jumps to the
-                        // end of its empty brick from here
-                        lat_out = Q.lat >= 0 ? Q.lat + j : -1;
-                        a_out = aj;
-                        advance_coarse(P, a_out, lat_out, Q.step, 1 + nskip);
-                        pre_out = 0.0f;
-                    }
+                    step_out = sj;
+                    lat_out = Q.lat >= 0 ? Q.lat + j + 1 : Q.lat;
                 } else if (refine_j) {              // refine before compositing sample j
-                    a_out = Q.step == L1 ? aj - (L1 - L4) : aj - (L4 - L8);
+                    a_out = sj == L1 ? aj - (L1 - L4) : aj - (L4 - L8);
                     pre_out = pre_j;
-                    step_out = Q.step == L1 ? L4 : L8;
+                    step_out = sj == L1 ? L4 : L8;
                     lat_out = -1;
                 } else {                            // sample j walked, then the step coarsens
                     a_out = aj + ns;
@@ -638,29 +668,33 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     step_out = ns;
                     lat_out = Q.lat >= 0 ? Q.lat + j + 1 : Q.lat;
                 }
-                const int src = g * G + (s_at < G ? s_at : G - 1);
+                const int src = g * G + (none ? r_hi : s_at);
                 const float a_new = __shfl_sync(FULL, a_out, src);
                 const float pre_new = __shfl_sync(FULL, pre_out, src);
                 const float step_new = __shfl_sync(FULL, step_out, src);
                 const int lat_new = __shfl_sync(FULL, lat_out, src);
                 if (simple) {
                     const CoopSample *gs = ws + g * G;
-                    const int n_comp = s_at == G ? G : (s_refine ? s_at : s_at + 1);
+                    // walked samples: sample 0 first if lead0, then [r_lo, c_end)
+                    const int c_end = none ? r_hi + 1 : (s_refine ? s_at : s_at + 1);
                     int c_lab = -1, c_slot = -2;
                     float c_cap = 0.0f, c_acc = 0.0f;
                     bool ended = false;
-                    float alpha_n = gs[0].alpha;
-                    int meta_n = gs[0].meta;
-                    float4 clr_n = gs[0].clr;
-                    for (int k = 0; k < n_comp; ++k) {
+                    int k = lead0 ? 0 : r_lo;
+                    float alpha_n = gs[k].alpha;
+                    int meta_n = gs[k].meta;
+                    float4 clr_n = gs[k].clr;
+                    while (k < c_end) {
                         const float alpha = alpha_n;
                         const int lab = (meta_n >> 4) & 255;
                         const float4 clr = clr_n;
-                        if (k + 1 < n_comp) {
-                            alpha_n = gs[k + 1].alpha;
-                            meta_n = gs[k + 1].meta;
-                            clr_n = gs[k + 1].clr;
+                        const int kn = (lead0 && k == 0) ? r_lo : k + 1;
+                        if (kn < c_end) {
+                            alpha_n = gs[kn].alpha;
+                            meta_n = gs[kn].meta;
+                            clr_n = gs[kn].clr;
                         }
+                        k = kn;
                         if (alpha > 0.0005f) {
                             if (lab != c_lab) {
                                 if (TRACK == kTrackShared && c_slot >= 0) s_acc[c_slot][owner_tid] = c_acc;
@@ -704,7 +738,10 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                 int meta = gs[0].meta;
                 float alpha_n = gs[0].alpha;
                 float4 clr_n = gs[0].clr;
-                while (k < G) {
+                // the lanes after sample 0 of a two-continuation round hold
+                // runs that start elsewhere: the walk takes sample 0 only
+                const int walk_end = two ? 1 : G;
+                while (k < walk_end) {
                     const int f = meta & 15;
                     if (f & kCoopEnd) {
                         Q.done = true;
@@ -713,7 +750,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     if (f & kCoopOutside) {
                         Q.a += Q.step;
                         if (Q.lat >= 0) ++Q.lat;
-                        if (++k < G) {
+                        if (++k < walk_end) {
                             meta = gs[k].meta;
                             alpha_n = gs[k].alpha;
                             clr_n = gs[k].clr;
@@ -725,7 +762,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                         Q.aPre = 0.0f;
                         advance_coarse(P, Q.a, Q.lat, Q.step, n);
                         k += n;
-                        if (k < G) {
+                        if (k < walk_end) {
                             meta = gs[k].meta;
                             alpha_n = gs[k].alpha;
                             clr_n = gs[k].clr;
@@ -736,7 +773,7 @@ __device__ void vr_coop_tail(const RayParams &P, cudaTextureObject_t vol, cudaTe
                     const float alpha = alpha_n;
                     const float4 clr = clr_n;
                     const int lab = (meta >> 4) & 255;
-                    if (k + 1 < G) {
+                    if (k + 1 < walk_end) {
                         meta = gs[k + 1].meta;
                         alpha_n = gs[k + 1].alpha;
                         clr_n = gs[k + 1].clr;
@@ -833,9 +870,9 @@ __device__ __forceinline__ float3 vr_light(const RayParams &P) {
 // MonkeyGL's d_render march (core/kernel.cu:156-256) for the ray of this
 // lane, called by every lane of the warp; returns the composited colour
 // (the background where nothing composited).
-template <int TRACK>
+template <int TRACK, int NT>
 __device__ __forceinline__ float4 vr_march(const RayParams &P, cudaTextureObject_t vol, cudaTextureObject_t mask,
-                                           const LabelSmem &S, const BrickView &BV, float (*s_acc)[256],
+                                           const LabelSmem &S, const BrickView &BV, float (*s_acc)[NT],
                                            CoopSample *ws, bool active, int x, int y) {
     const int tid = threadIdx.x;
     VrRay R;

@@ -220,6 +220,33 @@ def test_cpr_line_layer_in_vr(phantom):
     assert ((img == 255).all(-1)).sum() >= 100, "no CPR line drawn"
 
 
+# Before any label mask exists in MonkeyGL's process-wide state (see above).
+def test_text_annotations_in_vr(phantom):
+    """VR images with MonkeyGL's annotation layer: text of the three font
+    sizes and alignments, clipped at the image edges, drawn after the
+    orientation box (core/VRProvider.cpp:30-36, core/AnnotationLayer.cpp:41-61).
+    Both objects load their glyphs and mesh from oracle/_ref/resources."""
+    anns = [("annotation", "MonkeyGL B200 - VR 512x512", 6, 4, 0, 0, (1.0, 1.0, 0.0, 1.0)),
+            ("annotation", "WW/WL: 1700/650", 506, 30, 1, 1, (0.2, 0.9, 1.0, 1.0)),
+            ("annotation", "Axial {R} [x] ~`!@#$%^&*()", 256, 240, 2, 2, (1.0, 0.5, 0.25, 1.0)),
+            ("annotation", "edge clip", 480, 500, 2, 0, (0.9, 0.9, 0.9, 1.0)),
+            ("annotation", "left clip", -30, -10, 1, 0, (0.5, 1.0, 0.5, 1.0))]
+    ops = [("clear_annotations",), ("tf", TF4, {}, -1), ("wwwl", 1700, 650, -1), ("rotate", 25, 5)] + anns
+    try:
+        ref, mine = run_both(phantom, ops)
+        img = mine.GetVRImage()
+        assert_vr_equal(img, ref_vr(ref), "VR with text annotations")
+        # the text is there: the same view without annotations differs
+        L, h = ref.L, ref.h
+        L.mkrh_remove_annotations(h)
+        mine.RemoveAllAnnotations()
+        plain = mine.GetVRImage()
+        assert_vr_equal(plain, ref_vr(ref), "VR after removing the annotations")
+        assert int(np.count_nonzero((img != plain).any(-1))) > 500
+    finally:
+        RefHelloMonkey().L.mkrh_remove_annotations(RefHelloMonkey().h)
+
+
 @pytest.mark.parametrize("rtype", [0, 1, 2])
 def test_vr_through_the_api(phantom, rtype):
     ops = [("tf", TF4, {}, -1), ("wwwl", 1700, 650, -1), ("render_type", rtype), ("rotate", 30, 10),
@@ -275,28 +302,3 @@ def test_png_strings_decode_to_the_images(phantom):
     img = np.frombuffer(raw, np.uint8).reshape(h, 1 + w * 3)[:, 1:].reshape(h, w, 3)
     assert np.array_equal(img, mine.GetVRImage())
 
-
-def test_text_annotations_in_vr(phantom):
-    """VR images with MonkeyGL's annotation layer: text of the three font
-    sizes and alignments, clipped at the image edges, drawn after the
-    orientation box (core/VRProvider.cpp:30-36, core/AnnotationLayer.cpp:41-61).
-    Both objects load their glyphs and mesh from oracle/_ref/resources."""
-    anns = [("annotation", "MonkeyGL B200 - VR 512x512", 6, 4, 0, 0, (1.0, 1.0, 0.0, 1.0)),
-            ("annotation", "WW/WL: 1700/650", 506, 30, 1, 1, (0.2, 0.9, 1.0, 1.0)),
-            ("annotation", "Axial {R} [x] ~`!@#$%^&*()", 256, 240, 2, 2, (1.0, 0.5, 0.25, 1.0)),
-            ("annotation", "edge clip", 480, 500, 2, 0, (0.9, 0.9, 0.9, 1.0)),
-            ("annotation", "left clip", -30, -10, 1, 0, (0.5, 1.0, 0.5, 1.0))]
-    ops = [("clear_annotations",), ("tf", TF4, {}, -1), ("wwwl", 1700, 650, -1), ("rotate", 25, 5)] + anns
-    try:
-        ref, mine = run_both(phantom, ops)
-        img = mine.GetVRImage()
-        assert_vr_equal(img, ref_vr(ref), "VR with text annotations")
-        # the text is there: the same view without annotations differs
-        L, h = ref.L, ref.h
-        L.mkrh_remove_annotations(h)
-        mine.RemoveAllAnnotations()
-        plain = mine.GetVRImage()
-        assert_vr_equal(plain, ref_vr(ref), "VR after removing the annotations")
-        assert int(np.count_nonzero((img != plain).any(-1))) > 500
-    finally:
-        RefHelloMonkey().L.mkrh_remove_annotations(RefHelloMonkey().h)
