@@ -64,7 +64,7 @@ def parse_args():
     ap.add_argument("--mode", choices=["vr", "mip", "surface"], default="vr",
                     help="render type of the timed frames (the contract line is VR)")
     ap.add_argument("--suite", action="store_true")
-    ap.add_argument("--suite-only", default="", help="comma list of suite groups: vr,mpr,cpr,dvr,api (default all)")
+    ap.add_argument("--suite-only", default="", help="comma list of suite groups: vr,mip,mpr,cpr,dvr,api,upload (default all)")
     ap.add_argument("--serve", action="store_true", help="serving benchmark (monkeygl_b200.serve_bench)")
     ap.add_argument("--serve-requests", type=int, default=10000)
     ap.add_argument("--serve-rate", type=float, default=200.0)

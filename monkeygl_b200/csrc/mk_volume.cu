@@ -293,6 +293,265 @@ __global__ void __launch_bounds__(256) k_brick_labels_rows(const unsigned char *
     }
 }
 
+// ---------------------------------------------------------------------------
+// Brick maps from slices staged in shared memory.  Each block (one brick row
+// by, kZRun z-bricks) keeps kStages slices of its rows in flight: thread 0
+// issues one bulk copy per row (cp.async.bulk, global -> shared, completion
+// counted on the stage's mbarrier), every thread reads its brick's 16-byte
+// row segment and both halo voxels from shared memory, and the stage is
+// refilled with the slice kStages ahead once all threads have read it.  The
+// loads of a block so run ahead of its arithmetic by kStages slices whatever
+// the register count (the register-staged row kernels above wait on their
+// loads: ncu shows long-scoreboard stalls).  Waits are bounded: a stage that
+// does not complete within kStageWaitNs sets *err, and the block waits
+// (bounded again) for its own copies before it returns.
+constexpr int kStages = 4;
+constexpr unsigned long long kStageWaitNs = 200ull * 1000 * 1000;   // 200 ms
+
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// 16-byte aligned source, destination and size
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// true once phase `parity` of the barrier has completed; false after
+// kStageWaitNs (or 2^26 polls) without it
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    const unsigned long long t0 = global_ns();
+    for (int i = 0; i < (1 << 26); ++i) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 63) == 63 && global_ns() - t0 > kStageWaitNs) return false;
+    }
+    return false;
+}
+
+// Shared-memory bytes of the staged kernels: the barriers, then kStages
+// slices of `rows` rows of `row_bytes`.
+inline size_t staged_smem_bytes(int rows, size_t row_bytes) { return 128 + (size_t)kStages * rows * row_bytes; }
+
+// The staged kernels apply when rows are whole bricks of 16-byte multiples
+// and kStages slices fit in shared memory (dim_x up to about 2800).
+bool brick_minmax_staged_fit(int dim_x, int nbx) {
+    return dim_x % kBrick == 0 && nbx <= 256 && staged_smem_bytes(10, (size_t)dim_x * 2) <= 220 * 1024;
+}
+bool brick_labels_staged_fit(int dim_x, int nbx) {
+    return dim_x % 16 == 0 && nbx <= 256 && staged_smem_bytes(8, (size_t)dim_x) <= 220 * 1024;
+}
+
+__global__ void __launch_bounds__(256) k_brick_minmax_staged(const short *__restrict__ vox, int dx, int dy, int dz,
+                                                             int nbx, int nby, int nbz, short2 *out,
+                                                             unsigned *err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    const short *stage0 = reinterpret_cast<const short *>(smem + 128);
+    const size_t stage_elems = (size_t)10 * dx;
+    const unsigned row_bytes = (unsigned)dx * 2;
+    const int by = blockIdx.x;
+    const int bz0 = blockIdx.y * kZRun, bz1 = min(bz0 + kZRun, nbz);
+    const int za = max(bz0 * kBrick - 1, 0), zb = min(bz1 * kBrick, dz - 1);
+    const int nsl = zb - za + 1;
+    const size_t plane = (size_t)dx * dy;
+    auto issue = [&](int st, int z) {        // thread 0: slice z into stage st
+        uint64_t *bar = &bars[st];
+        mbar_expect_tx(bar, 10u * row_bytes);
+        unsigned char *dst = smem + 128 + (size_t)st * stage_elems * 2;
+        for (int r = 0; r < 10; ++r) {
+            const int y = min(max(by * kBrick - 1 + r, 0), dy - 1);
+            bulk_to_smem(dst + (size_t)r * row_bytes, vox + (size_t)z * plane + (size_t)y * dx, row_bytes, bar);
+        }
+    };
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kStages; ++st) mbar_init(&bars[st], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < kStages && i < nsl; ++i) issue(i, za + i);
+    const int lane = threadIdx.x & 31;
+    const int bx = min((int)threadIdx.x, nbx - 1);
+    const bool owner = (int)threadIdx.x < nbx;
+    const int x0 = bx * kBrick;
+    const bool left = bx > 0, right = bx + 1 < nbx;
+    Mm8 acc, prev;
+    mm8_init(acc);
+    mm8_init(prev);
+    int cur = bz0;
+    bool failed = false;
+    int i = 0;
+    for (; i < nsl; ++i) {
+        const int st = i % kStages;
+        const bool ok = mbar_wait(&bars[st], (unsigned)(i / kStages) & 1u);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        const short *sl = stage0 + (size_t)st * stage_elems;
+        Mm8 S;
+        mm8_init(S);
+#pragma unroll
+        for (int r = 0; r < 10; ++r) {
+            const short *row = sl + (size_t)r * dx;
+            const uint4 v = *reinterpret_cast<const uint4 *>(row + x0);
+            S.lo.x = __vmins2(S.lo.x, v.x);
+            S.lo.y = __vmins2(S.lo.y, v.y);
+            S.lo.z = __vmins2(S.lo.z, v.z);
+            S.lo.w = __vmins2(S.lo.w, v.w);
+            S.hi.x = __vmaxs2(S.hi.x, v.x);
+            S.hi.y = __vmaxs2(S.hi.y, v.y);
+            S.hi.z = __vmaxs2(S.hi.z, v.z);
+            S.hi.w = __vmaxs2(S.hi.w, v.w);
+            // x halo from the neighbouring lanes, as mm8_slice (lanes 0 and 31 read it)
+            int l = (short)(__shfl_up_sync(0xffffffffu, v.w, 1) >> 16);
+            int h = (short)(__shfl_down_sync(0xffffffffu, v.x, 1) & 0xffffu);
+            if (lane == 0 && left) l = row[x0 - 1];
+            if (lane == 31 && right) h = row[x0 + 8];
+            if (!left) l = (short)(v.x & 0xffffu);
+            if (!right) h = (short)(v.w >> 16);
+            S.hlo = min(S.hlo, min(l, h));
+            S.hhi = max(S.hhi, max(l, h));
+        }
+        __syncthreads();                      // every thread has read stage st
+        if (threadIdx.x == 0 && i + kStages < nsl) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(st, za + i + kStages);
+        }
+        const int z = za + i;
+        mm8_merge(acc, S);
+        if ((z >> kBrickShift) > cur) {       // z = 8 (cur + 1): the slice above brick cur
+            if (owner) out[((size_t)cur * nby + by) * nbx + bx] = mm8_result(acc);
+            ++cur;
+            acc = prev;                       // the slice below brick cur, then its first slice
+            mm8_merge(acc, S);
+        }
+        prev = S;
+    }
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1u);
+            // copies in flight: stages i .. min(i + kStages, nsl) - 1; wait for them (bounded)
+            for (int k = i; k < nsl && k < i + kStages; ++k) mbar_wait(&bars[k % kStages], (unsigned)(k / kStages) & 1u);
+        }
+        __syncthreads();
+        return;
+    }
+    // the loop reads every issued slice (it stops at the slice above brick
+    // bz1 - 1, the last one staged), so no copy is in flight here
+    if (cur < bz1 && owner) out[((size_t)cur * nby + by) * nbx + bx] = mm8_result(acc);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_brick_labels_staged(const unsigned char *__restrict__ lab, int dx, int dy,
+                                                             int dz, int nbx, int nby, int nbz, uint32_t *out,
+                                                             uint32_t *present, unsigned *err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    const size_t stage_bytes = (size_t)8 * dx;
+    const int by = blockIdx.x;
+    const int bz0 = blockIdx.y * kZRun, bz1 = min(bz0 + kZRun, nbz);
+    const int z0 = bz0 * kBrick, z1 = min(bz1 * kBrick, dz);   // slices [z0, z1)
+    const int nsl = z1 - z0;
+    const int y0 = by * kBrick, ny = min(kBrick, dy - y0);
+    const size_t plane = (size_t)dx * dy;
+    auto issue = [&](int st, int z) {
+        uint64_t *bar = &bars[st];
+        mbar_expect_tx(bar, (unsigned)(ny * dx));
+        unsigned char *dst = smem + 128 + (size_t)st * stage_bytes;
+        for (int r = 0; r < ny; ++r)
+            bulk_to_smem(dst + (size_t)r * dx, lab + (size_t)z * plane + (size_t)(y0 + r) * dx, (unsigned)dx, bar);
+    };
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < kStages; ++st) mbar_init(&bars[st], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int i = 0; i < kStages && i < nsl; ++i) issue(i, z0 + i);
+    const int bx = threadIdx.x;
+    const bool owner = bx < nbx;
+    const int x0 = (owner ? bx : 0) * kBrick;
+    uint32_t m0 = 0, m1 = 0, m2 = 0, p0 = 0, p1 = 0, p2 = 0;
+    bool failed = false;
+    int i = 0;
+    for (; i < nsl; ++i) {
+        const int st = i % kStages;
+        const bool ok = mbar_wait(&bars[st], (unsigned)(i / kStages) & 1u);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        if (owner) {
+            const unsigned char *sl = smem + 128 + (size_t)st * stage_bytes;
+            for (int r = 0; r < ny; ++r) {
+                const uint2 w = *reinterpret_cast<const uint2 *>(sl + (size_t)r * dx + x0);
+                label_bits_word(w.x, m0, m1, m2);
+                label_bits_word(w.y, m0, m1, m2);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && i + kStages < nsl) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(st, z0 + i + kStages);
+        }
+        const int z = z0 + i;
+        if (((z + 1) & (kBrick - 1)) == 0 || z + 1 == z1) {   // last slice of brick z >> 3
+            if (owner) {
+                uint32_t *o = out + 3 * (((size_t)(z >> kBrickShift) * nby + by) * nbx + bx);
+                o[0] = m0;
+                o[1] = m1;
+                o[2] = m2;
+            }
+            p0 |= m0;
+            p1 |= m1;
+            p2 |= m2;
+            m0 = m1 = m2 = 0;
+        }
+    }
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, 1u);
+            for (int k = i; k < nsl && k < i + kStages; ++k) mbar_wait(&bars[k % kStages], (unsigned)(k / kStages) & 1u);
+        }
+        __syncthreads();
+        return;
+    }
+    if (!owner) p0 = p1 = p2 = 0;
+    p0 = __reduce_or_sync(0xffffffffu, p0);
+    p1 = __reduce_or_sync(0xffffffffu, p1);
+    p2 = __reduce_or_sync(0xffffffffu, p2);
+    if ((threadIdx.x & 31) == 0 && (p0 | p1 | p2)) {
+        atomicOr(&present[0], p0);
+        atomicOr(&present[1], p1);
+        atomicOr(&present[2], p2);
+    }
+}
+
 __global__ void k_fill_labels_zero(uint32_t *out, int nbricks) {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b < nbricks) {
@@ -621,7 +880,17 @@ extern "C" int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x
         st.device_bytes += nbricks * (sizeof(short2) + 3 * sizeof(uint32_t) + sizeof(float)) +
                            nwords * sizeof(uint32_t) + sizeof(unsigned long long);
         cudaMemsetAsync(st.d_visible, 0, nwords * sizeof(uint32_t), st.stream);
-        if (brick_rows_fit(dim_x, st.nb[0])) {
+        const bool staged = brick_minmax_staged_fit(dim_x, st.nb[0]);
+        if (staged) {
+            // d_counter doubles as the staged kernel's wait-timeout flag until the first render
+            const size_t smem = staged_smem_bytes(10, (size_t)dim_x * 2);
+            const dim3 grid(st.nb[1], (st.nb[2] + kZRun - 1) / kZRun);
+            cudaMemsetAsync(st.d_counter, 0, sizeof(unsigned long long), st.stream);
+            cudaFuncSetAttribute(k_brick_minmax_staged, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            k_brick_minmax_staged<<<grid, (st.nb[0] + 31) & ~31, smem, st.stream>>>(
+                (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], st.nb[2], st.d_minmax,
+                reinterpret_cast<unsigned *>(st.d_counter));
+        } else if (brick_rows_fit(dim_x, st.nb[0])) {
             const dim3 grid(st.nb[1], (st.nb[2] + kZRun - 1) / kZRun);
             k_brick_minmax_rows<<<grid, (st.nb[0] + 31) & ~31, 0, st.stream>>>(
                 (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], st.nb[2], st.d_minmax);
@@ -659,10 +928,18 @@ extern "C" int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x
         st.device_bytes += accu.size() * sizeof(float);
         e = cudaMemcpyAsync(st.d_accu, accu.data(), accu.size() * sizeof(float),
                             cudaMemcpyHostToDevice, st.stream);
+        unsigned long long timed_out = 0;
+        if (e == cudaSuccess && staged)
+            e = cudaMemcpyAsync(&timed_out, st.d_counter, sizeof(timed_out), cudaMemcpyDeviceToHost, st.stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st.stream);
         if (e != cudaSuccess) {
             set_last_error(std::string("mk_volume_create: ") + cudaGetErrorString(e));
             rc = MK_ERR_CUDA;
+            break;
+        }
+        if (timed_out) {
+            set_last_error("mk_volume_create: brick min/max staging timed out");
+            rc = MK_ERR_TIMEOUT;
             break;
         }
     } while (0);
@@ -809,20 +1086,30 @@ extern "C" int mk_volume_set_mask(mk_volume v, const uint8_t *labels) {
     // labels present anywhere (used to size per-ray state): OR-ed on the
     // device by the row kernel, else scanned on the host
     const bool rows = brick_rows_fit(dx, st.nb[0]);
-    uint32_t h_present[3] = {0, 0, 0};
+    const bool staged = brick_labels_staged_fit(dx, st.nb[0]);
+    uint32_t h_present[4] = {0, 0, 0, 0};   // label bits 0..64, then the staged kernel's timeout flag
     uint32_t *d_present = nullptr;
-    if (rc == MK_OK && rows && cudaMalloc(&d_present, 3 * sizeof(uint32_t)) != cudaSuccess) {
+    if (rc == MK_OK && rows && cudaMalloc(&d_present, sizeof(h_present)) != cudaSuccess) {
         cudaGetLastError();
         set_last_error("mk_volume_set_mask: allocation failed");
         rc = MK_ERR_OUT_OF_MEMORY;
     }
     if (rc == MK_OK) {
         if (rows) {
-            e = cudaMemsetAsync(d_present, 0, 3 * sizeof(uint32_t), st.stream);
+            e = cudaMemsetAsync(d_present, 0, sizeof(h_present), st.stream);
             const dim3 grid(st.nb[1], (st.nb[2] + kZRun - 1) / kZRun);
-            if (e == cudaSuccess)
+            if (e == cudaSuccess && staged) {
+                const size_t smem = staged_smem_bytes(8, (size_t)dx);
+                e = cudaFuncSetAttribute(k_brick_labels_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+                if (e == cudaSuccess)
+                    k_brick_labels_staged<<<grid, (st.nb[0] + 31) & ~31, smem, st.stream>>>(
+                        (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], st.nb[2], st.d_labels,
+                        d_present, d_present + 3);
+            } else if (e == cudaSuccess) {
                 k_brick_labels_rows<<<grid, (st.nb[0] + 31) & ~31, 0, st.stream>>>(
                     (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], st.nb[2], st.d_labels, d_present);
+            }
         } else {
             k_brick_labels<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
                 (const unsigned char *)d_lin, dx, dy, dz, st.nb[0], st.nb[1], (int)nbricks, st.d_labels);
@@ -834,6 +1121,9 @@ extern "C" int mk_volume_set_mask(mk_volume v, const uint8_t *labels) {
         if (e != cudaSuccess) {
             set_last_error(std::string("mk_volume_set_mask: ") + cudaGetErrorString(e));
             rc = MK_ERR_CUDA;
+        } else if (h_present[3]) {
+            set_last_error("mk_volume_set_mask: brick label staging timed out");
+            rc = MK_ERR_TIMEOUT;
         }
     }
     cudaFree(d_present);

@@ -22,8 +22,18 @@ from __future__ import annotations
 
 import json
 import queue
+import sys
 import threading
 import time
+
+
+def _phase(what, t0=[None]):
+    """Progress of the benchmark's phases on stderr (the result line goes
+    to stdout at the end)."""
+    now = time.perf_counter()
+    if t0[0] is None:
+        t0[0] = now
+    print(f"[serve_bench {now - t0[0]:8.1f} s] {what}", file=sys.stderr, flush=True)
 
 import numpy as np
 
@@ -62,6 +72,34 @@ def _pcts(lat):
             "mean_ms": round(float(a.mean()), 3), "max_ms": round(float(a.max()), 3)}
 
 
+# A request not done this long after the collector starts waiting for it
+# ends the run with MK_ERR_TIMEOUT instead of waiting for good.
+WAIT_LIMIT_MS = 120_000
+
+
+def eviction_trace(trace, n, pairs):
+    """`n` requests of `trace` in len(pairs) phases of equal length: phase k
+    takes, in trace order, the next requests whose volume is in pairs[k] (a
+    reader who finishes one pair of studies and opens the next).  Arrival
+    gaps are the trace's own, so the rate is unchanged."""
+    from dataclasses import replace
+    per = -(-n // len(pairs))
+    out, t, used = [], 0.0, set()
+    gaps = [r.arrival_s - (trace[i - 1].arrival_s if i else 0.0) for i, r in enumerate(trace)]
+    for k, pair in enumerate(pairs):
+        taken = 0
+        for i, r in enumerate(trace):
+            if taken == per or len(out) == n:
+                break
+            if i in used or r.volume not in pair:
+                continue
+            used.add(i)
+            t += gaps[len(out)]
+            out.append(replace(r, arrival_s=t))
+            taken += 1
+    return out
+
+
 def run_server(srv, vids, trace, pool, open_loop: bool):
     """Submit the trace (at its arrival times if open_loop, else at once);
     returns per-request latencies (ms), wall seconds and the images' tickets order."""
@@ -91,7 +129,7 @@ def run_server(srv, vids, trace, pool, open_loop: bool):
         if item is None:
             break
         i, t, b, sub_wall = item
-        _, tm = srv.wait(t)
+        _, tm = srv.wait(t, WAIT_LIMIT_MS)
         pool.give(b)
         late = max(0.0, sub_wall - (t0 + trace[i].arrival_s)) * 1e3 if open_loop else (sub_wall - t0) * 1e3
         lat[i] = late + (tm["completed_ms"] - tm["submitted_ms"])
@@ -169,11 +207,14 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True)
 
     nsat = min(n, nsat)
     torch.cuda.init()
+    _phase("phantoms")
     if phantoms is None:
         phantoms = serving_phantoms()
     specs = [(p.dims, p.spacing, p.labels is not None) for p in phantoms]
+    _phase("trace")
     trace = serving_trace(specs, n, rate, seed=2024)
     pool = _Pool(64, 1024 * 1024 * 4)
+    _phase("server and volumes")
 
     srv = S.Server(max_slots=32, max_pending=max(n, 1), max_pixels=1024 * 1024, max_labels=8)
     slot_bytes = srv.stats()["resident_bytes"]
@@ -189,6 +230,7 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True)
             v.set_mask(p.labels)
         plain_vols.append(v)
 
+    _phase("warm-up")
     # warm-up: every volume and kind once on both paths; spot-check equality
     warm = serving_trace(specs, 64, 1000.0, seed=99)
     bad = []
@@ -210,10 +252,14 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True)
         raise RuntimeError(f"server and plain path images differ on {len(bad)} of {len(warm)} requests")
 
     st0 = srv.stats()
+    _phase("server, open loop")
     lat_s, wall_s = run_server(srv, vids, trace, pool, open_loop=True)
     st1 = srv.stats()
+    _phase("plain path, open loop")
     lat_p, wall_p = run_plain(plain_vols, trace, pool, open_loop=True)
+    _phase("server, saturation")
     sat_s_lat, sat_s = run_server(srv, vids, trace[:nsat], pool, open_loop=False)
+    _phase("plain path, saturation")
     sat_p_lat, sat_p = run_plain(plain_vols, trace[:nsat], pool, open_loop=False)
     srv.close()
     for v in plain_vols:
@@ -241,7 +287,9 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True)
             ref.select(i + 1)
             ref.set_volume(p.volume)
             ref.set_mask(p.labels)
+        _phase("MonkeyGL path, open loop")
         lat_m, wall_m = run_monkeygl(ref, trace, pool, open_loop=True)
+        _phase("MonkeyGL path, saturation")
         sat_m_lat, sat_m = run_monkeygl(ref, trace[:nsat], pool, open_loop=False)
         ref.select(0)
         line["monkeygl_plain"] = {**_pcts(lat_m), "renders_per_s": round(n / wall_m, 1),
@@ -249,19 +297,29 @@ def measure(n=10000, rate=200.0, nsat=2000, phantoms=None, ref=None, evict=True)
         line["saturation_ratio_vs_monkeygl"] = round((nsat / sat_s) / (nsat / sat_m), 2)
         line["saturation_latency"]["monkeygl_plain"] = _pcts(sat_m_lat)
     if evict:
-        # the budget holds the slots and 70% of the four volumes: requests for
-        # an evicted volume wait for its upload while the others keep running
-        budget = int(slot_bytes + 0.7 * sum(vol_bytes))
+        # The budget holds the slots and the two largest volumes, not all
+        # four; the requests move between pairs of volumes in phases.  Each
+        # phase change evicts the idle volume that the new pair does not use
+        # and uploads the one it needs, while requests for the other keep
+        # running.  (A budget below the volumes that the requests of any one
+        # second use makes every path thrash: each request waits for an upload.)
+        big = sorted(range(len(vol_bytes)), key=lambda i: -vol_bytes[i])
+        budget = int(slot_bytes + vol_bytes[big[0]] + vol_bytes[big[1]])
+        nv = len(phantoms)
+        pairs = [(k % nv, (k + 1) % nv) for k in range(nv)]
         ne = min(n, 2000)
+        etrace = eviction_trace(trace, ne, pairs)
+        _phase("eviction run")
         with S.Server(max_slots=32, max_pending=max(ne, 1), max_pixels=1024 * 1024, max_labels=8,
                       hbm_budget_bytes=budget, evict_idle=True) as es:
             evids = [es.add_volume(p.volume, p.labels) for p in phantoms]
-            lat_e, wall_e = run_server(es, evids, trace[:ne], pool, open_loop=True)
+            lat_e, wall_e = run_server(es, evids, etrace, pool, open_loop=True)
             est = es.stats()
-        line["eviction"] = {**_pcts(lat_e), "requests": ne, "renders_per_s": round(ne / wall_e, 1),
-                            "budget_mb": round(budget / 2 ** 20, 1),
+        line["eviction"] = {**_pcts(lat_e), "requests": len(etrace), "renders_per_s": round(len(etrace) / wall_e, 1),
+                            "phases": [list(p) for p in pairs], "budget_mb": round(budget / 2 ** 20, 1),
                             "volumes_mb": round(sum(vol_bytes) / 2 ** 20, 1),
                             "evictions": est["evictions"], "loads": est["loads"]}
+    _phase("done")
     return line
 
 

@@ -2,6 +2,7 @@
 
 Rows (synthetic seeded phantoms of monkeygl_b200.phantom):
   * VR and MIP of the cardiac phantom (int16 512x512x361) at 1024^2, 36 views;
+  * MIP of the body phantom at 1024^2;
   * VR of the body phantom (int16 512x512x1559, 4 labels) at 1024^2 with
     background opacity caps 0.4 and 0.8;
   * MPR of the cardiac phantom: axial, sagittal, coronal and 8 seeded oblique
@@ -13,7 +14,8 @@ Rows (synthetic seeded phantoms of monkeygl_b200.phantom):
   * differentiable VR: float32 256^3 volume, 256-entry LUT, 8 views of 256^2,
     step 0.5 voxel -- forward, backward and their ratio;
   * GetVRData through the HelloMonkey API (render, orientation box, copy
-    back), 512x512, 36 views, beside MonkeyGL's complete HelloMonkey path.
+    back), 512x512, 36 views, beside MonkeyGL's complete HelloMonkey path;
+  * upload of the body volume and its labels (brick maps included).
 
 Device times are CUDA events on the launching stream around each call, L2
 flushed (256 MiB write) between calls outside the events, median over the
@@ -326,6 +328,35 @@ def api_rows(ctx):
     return [row]
 
 
+def upload_rows(ctx):
+    """Upload of the body volume and its labels: mk_volume_create (3D array
+    copy, brick min/max, schedule table) + mk_volume_set_mask (mask texture,
+    brick label sets), wall clock from host arrays, beside MonkeyGL's
+    SetVolumeData + SetMask of the same arrays (its CuDataManager copies the
+    volume into a 3D array and the mask into another)."""
+    from monkeygl_b200 import capi
+    w = _workload(ctx, "body")
+    vox, lab = w.phantom.volume, w.phantom.labels
+
+    def ours(_):
+        v = capi.Volume(vox)
+        v.set_mask(lab)
+        v.close()
+
+    ours(0)
+    row = {"row": "upload body volume + labels", "image": "x".join(map(str, vox.shape[::-1])),
+           "e2e_ms": round(_wall_ms(ours, 5), 2)}
+    ref = ctx["ref"]
+    if ref is not None:
+        def theirs(_):
+            ref.set_volume(vox)
+            ref.set_mask(lab)
+        theirs(0)
+        row["ref_call_ms"] = round(_wall_ms(theirs, 5), 2)
+        row["speedup_e2e"] = round(row["ref_call_ms"] / row["e2e_ms"], 2)
+    return [row]
+
+
 def main(args=None, ref=None, ref_api=None, resources_dir=None):
     """Print the table.  `ref` is MonkeyGL's own CUDA path (an object with
     set_volume / set_mask / clear_tfs / set_lut / kernel_ms / plane / cpr),
@@ -341,10 +372,13 @@ def main(args=None, ref=None, ref_api=None, resources_dir=None):
     want = lambda g: not only or g in only
     rows = []
     if want("vr"):
-        rows += vr_rows("cardiac", 0.4, (0, 1), ctx)
+        rows += vr_rows("cardiac", 0.4, (0,), ctx)
         rows += vr_rows("body", 0.4, (0,), ctx)
         rows += vr_rows("body", 0.8, (0,), ctx)
         rows += vr_rows("body", 0.4, (0,), ctx, dense=True)
+    if want("mip"):
+        rows += vr_rows("cardiac", 0.4, (1,), ctx)
+        rows += vr_rows("body", 0.4, (1,), ctx)
     if want("mpr"):
         rows += mpr_rows(ctx)
     if want("cpr"):
@@ -353,6 +387,8 @@ def main(args=None, ref=None, ref_api=None, resources_dir=None):
         rows += dvr_rows(ctx)
     if want("api"):
         rows += api_rows(ctx)
+    if want("upload"):
+        rows += upload_rows(ctx)
     for r in rows:
         print(json.dumps(r), flush=True)
     keys = ["row", "image", "ms", "e2e_ms", "ref_kernel_ms", "ref_call_ms", "speedup_kernel", "speedup_e2e",

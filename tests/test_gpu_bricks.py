@@ -86,7 +86,8 @@ def test_brick_maps_body():
     check_maps(w.phantom.volume, w.phantom.labels, "body")
 
 
-@pytest.mark.parametrize("dims", [(100, 90, 70), (64, 60, 45), (8, 8, 8), (7, 3, 2), (2048, 16, 9)])
+@pytest.mark.parametrize("dims", [(100, 90, 70), (64, 60, 45), (8, 8, 8), (7, 3, 2), (2048, 16, 9),
+                                  (200, 40, 33), (24, 20, 17)])
 def test_brick_maps_shapes(dims):
     X, Y, Z = dims
     rng = np.random.default_rng(X * 7 + Y * 3 + Z)
