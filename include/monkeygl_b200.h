@@ -147,6 +147,9 @@ const char *mk_version(void);
  * thread at a time (its per-frame caches -- tile orders, ray parameter
  * tables, hand-off lists -- are not locked); concurrent renders of one volume
  * go through several streams from that thread, or through mk_server_*.
+ * The brick maps are built by kernels whose waits are bounded: a wait that
+ * runs out (never expected) is reported as MK_ERR_TIMEOUT and no volume is
+ * returned.
  */
 int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x, int dim_y,
                      int dim_z, int device);
@@ -171,7 +174,8 @@ int mk_volume_brick_maps(mk_volume vol, int *nb, int16_t *minmax, uint32_t *labe
 /*
  * Upload (labels != NULL) or remove (labels == NULL) the uint8 label volume,
  * same dims and layout as the voxels.  Replaces cu_copyMaskData
- * (core/CuDataManager.cu:75-120).
+ * (core/CuDataManager.cu:75-120).  MK_ERR_TIMEOUT as for mk_volume_create
+ * (the label sets' bounded waits); the volume then has no mask.
  */
 int mk_volume_set_mask(mk_volume vol, const uint8_t *labels);
 

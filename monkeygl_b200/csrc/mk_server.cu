@@ -149,7 +149,7 @@ struct Slot {
 
 struct ServerVolume {
     mk_volume vol = nullptr;            // nullptr while evicted (or being uploaded)
-    size_t bytes = 0;                   // device bytes while resident, else the estimate
+    size_t bytes = 0;                   // device bytes while resident; evicted: those of its last upload (the estimate if none)
     int users = 0;                      // requests queued or in flight
     int in_slots = 0;                   // requests admitted into slots: they pin the volume
     bool loading = false;               // queued for, or in, an upload by the loader thread
@@ -649,7 +649,11 @@ void loader_loop(mk_server_s *s) {
             continue;
         }
         ServerVolume &V = it->second;
-        const size_t est = volume_estimate(V.dims[0], V.dims[1], V.dims[2], V.host_lab != nullptr);
+        // the device bytes of its previous upload (an evicted volume keeps
+        // them), or the estimate for one never uploaded: an estimate above
+        // the real size would make two volumes that fit the budget together
+        // look as if they did not, and every switch between them an eviction
+        const size_t est = V.bytes;
         std::vector<int> victims = eviction_victims(s, id, est);
         if (s->resident + est > s->budget && victims.empty()) {
             // every resident volume is in use: wait for requests to retire
@@ -662,8 +666,7 @@ void loader_loop(mk_server_s *s) {
             ServerVolume &E = s->volumes[vid];
             dead.push_back(E.vol);
             E.vol = nullptr;
-            s->resident -= E.bytes;
-            E.bytes = volume_estimate(E.dims[0], E.dims[1], E.dims[2], E.host_lab != nullptr);
+            s->resident -= E.bytes;             // E.bytes stays: the size of its next upload
             s->stats.evictions++;
         }
         s->resident += est;                     // reserved while uploading
@@ -938,8 +941,7 @@ extern "C" int mk_server_add_volume(mk_server s, const int16_t *voxels, int dim_
                 ServerVolume &E = s->volumes[vid];
                 dead.push_back(E.vol);
                 E.vol = nullptr;
-                s->resident -= E.bytes;
-                E.bytes = volume_estimate(E.dims[0], E.dims[1], E.dims[2], E.host_lab != nullptr);
+                s->resident -= E.bytes;         // E.bytes stays: the size of its next upload
                 s->stats.evictions++;
             }
         }
