@@ -441,6 +441,26 @@ int tracking_mode_for(const uint64_t present[2], const float (*params)[3]) {
 
 static int tracking_mode(const VolumeState &v) { return tracking_mode_for(v.present_labels, v.params); }
 
+// MIP takes the uniform-window loop when every label present in the mask
+// has alpha > 0 and all of them share one window with ww > 0.
+void set_mip_window(RayParams &P, const uint64_t present[2], const float (*params)[3]) {
+    P.mip_uniform = 0;
+    int first = -1;
+    for (int l = 0; l < MK_MAX_LABELS; ++l) {
+        if (!((present[l >> 6] >> (l & 63)) & 1ull)) continue;
+        if (!(params[l][0] > 0.0f)) return;
+        if (first < 0) {
+            first = l;
+        } else if (params[l][1] != params[first][1] || params[l][2] != params[first][2]) {
+            return;
+        }
+    }
+    if (first < 0 || !(params[first][1] > 0.0f)) return;
+    P.mip_uniform = 1;
+    P.mip_ww = params[first][1];
+    P.mip_wl = params[first][2];
+}
+
 int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P) {
     if (!p || p->width <= 0 || p->height <= 0 || p->width > 16384 || p->height > 16384) {
         set_last_error("mk_render_vr: image size must be in [1, 16384]");
@@ -485,6 +505,9 @@ int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P) {
     P.spill = nullptr;
     P.spill_cap = 0;
     P.tail_trigger = 0;
+    P.mip_uniform = 0;
+    P.mip_ww = 1.0f;
+    P.mip_wl = 0.0f;
     return MK_OK;
 }
 
@@ -521,6 +544,7 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     rc = fy_table(v, P.scale, s, &P.fy_tab, &fy_idx);
     if (rc != MK_OK) return rc;
     const int track = tracking_mode(v);
+    if (params->render_type == MK_RENDER_MIP) set_mip_window(P, v.present_labels, v.params);
     const bool tail = params->render_type == MK_RENDER_VR && track != kTrackLocal &&
                       !(params->flags & (MK_VR_NO_TAIL | MK_VR_NO_COOP));
     if (tail) {

@@ -60,6 +60,11 @@ struct RayParams {
     SpillRay *spill;             // rays handed to the tail launch
     int spill_cap;
     int tail_trigger;            // rays still marching spill once this many tiles have finished
+    // MIP: 1 when every label present in the mask is visible (alpha > 0) and
+    // shares one window (mip_ww > 0, mip_wl); the label fetch is then not
+    // needed and the window is applied only to a new raw maximum
+    int mip_uniform;
+    float mip_ww, mip_wl;
 };
 
 struct LabelSmem {
@@ -1100,6 +1105,53 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                     if (A > 0.995f) break;
                 }
                 if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;
+            } else if (MODE == kModeMIP && !COUNT && P.mip_uniform) {
+                // Every label the ray can meet is visible and has the same
+                // window w(t) = (32768 t - wl) / ww + 0.5 with ww > 0.  Each of
+                // its operations is rounded monotonically (a product by a
+                // power of two, a difference, a quotient by a positive
+                // number, a sum), so w is non-decreasing and the maximum of
+                // w over the samples is w of the largest raw sample: the
+                // label fetch is dropped and w is evaluated only when a
+                // sample exceeds the raw maximum so far.  A holds the same
+                // value as in the general loop below after every sample.
+                int k = k0;
+                float vmax = -INFINITY;
+                while (a < P.limit) {
+                    if (a > a_stop) break;
+                    const float3 pos = ray_pos_at<false>(P, u, v, k, a);
+                    const int ix = pos.x * P.fdim[0];
+                    const int iy = pos.y * P.fdim[1];
+                    const int iz = pos.z * P.fdim[2];
+                    if (outside_voi(P, ix, iy, iz)) {
+                        k = min(k + 1, P.accu_len - 1);
+                        a = P.accu[k];
+                        continue;
+                    }
+                    if (P.skip) {
+                        const int b = brick_index(P, BV, ix, iy, iz);
+                        if (BV.mip_tmax[b] <= A) {
+                            const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1],
+                                                          pos.z * P.fdim[2]);
+                            k = min(k + 1 + steps_in_brick(pv, dv, ix, iy, iz), P.accu_len - 1);
+                            a = P.accu[k];
+                            continue;
+                        }
+                    }
+                    const float raw = tex3D<float>(vol, pos.x, pos.y, pos.z);
+                    if (raw > vmax) {
+                        vmax = raw;
+                        float temp = 32768 * raw;
+                        temp = (temp - P.mip_wl) / P.mip_ww + 0.5f;
+                        if (A < temp) A = temp;
+                    }
+                    k = min(k + 1, P.accu_len - 1);
+                    a = P.accu[k];
+                    // the output saturates at 1.0 (core/kernel.cu:351-358)
+                    if (P.skip && A >= 1.0f) break;
+                }
+                if (A <= 0.0f) sum = P.bg;
+                else sum = make_float4(A, A, A, A);
             } else if (MODE == kModeMIP) {
                 // fixed step 1/dim_z from a table entry: every sample is
                 // table entry k, a == accu[k]
@@ -1266,6 +1318,9 @@ int fy_table(VolumeState &v, float scale, cudaStream_t s, const float **out, int
 // Host: build that table into `out` (v.accu_len floats) on stream s.
 int launch_fy_table(const VolumeState &v, float scale, float *out, cudaStream_t s);
 int tracking_mode_for(const uint64_t present[2], const float (*params)[3]);
+// Host: P.mip_uniform / mip_ww / mip_wl for the labels present in a volume
+// under a table of (alpha, ww, wl) rows.
+void set_mip_window(RayParams &P, const uint64_t present[2], const float (*params)[3]);
 // Host: the 32x8 tiles of a W x H frame (index by * tiles_x + bx) sorted by
 // the distance of their centre to (W/2 + xT, H/2 + yT), where the volume
 // centre projects: launching them in this order starts the long rays first.

@@ -338,6 +338,7 @@ int admit(mk_server_s *s, uint64_t ticket, int slot_index) {
             D.lt.wl[l] = params[l][2];
         }
         D.track = tracking_mode_for(vs.present_labels, params);
+        if (q.r.kind == MK_REQUEST_MIP) set_mip_window(D.rp, vs.present_labels, params);
         D.vol = vs.tex_linear;
         D.mask = vs.tex_mask;
         const float *alpha_ptr[MK_MAX_LABELS];

@@ -194,6 +194,46 @@ def test_multilabel_matches_reference(ref, labelled, bg):
     v.close()
 
 
+def test_mip_label_windows_match_reference(ref, labelled):
+    """MIP takes a loop without label fetches when every label present is
+    visible and all of them share one window with a positive width (the
+    window is monotonic, so the maximum of the windowed samples is the
+    window of the largest raw sample); per-label windows or a hidden label
+    take the general loop (widths are positive: mk_volume_set_label_params
+    refuses others).  Every variant equals
+    MonkeyGL's image (core/kernel.cu:326-364), with and without skipping."""
+    w = labelled
+    v = capi.Volume(w.phantom.volume)
+    v.set_mask(w.phantom.labels)
+    for l, lut in w.luts.items():
+        v.set_transfer_function(l, lut)
+    load_ref(ref, w)
+    base = w.label_params.copy()
+    variants = [("uniform", base)]
+    lp = base.copy()
+    lp[2, 1:] = (900.0, 300.0)
+    variants.append(("per-label window", lp))
+    lp = base.copy()
+    lp[3, 0] = 0.0
+    variants.append(("hidden label", lp))
+    lp = base.copy()
+    lp[0, 0] = 0.0
+    variants.append(("hidden background", lp))
+    lp = base.copy()
+    lp[:5, 1:] = (400.0, 40.0)
+    variants.append(("uniform narrow window", lp))
+    for name, lp in variants:
+        v.set_label_params(lp)
+        for ang in (0.0, 70.0, 200.0):
+            p = params(w, ang, 1, size=256)
+            r = ref.render(256, 256, 1, capi.vr_params_flat(p, lp))
+            m = v.render_vr(p)
+            assert_image_parity(m, r, f"mip {name} {ang}", exact=True)
+            p.flags = capi.VR_NO_SKIP
+            assert np.array_equal(v.render_vr(p), m), f"mip {name} {ang} without skipping"
+    v.close()
+
+
 def test_cardiac_frame_matches_reference(ref):
     w = wl.make_workload("cardiac")
     v = capi.Volume(w.phantom.volume)
