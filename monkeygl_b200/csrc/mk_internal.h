@@ -140,6 +140,14 @@ struct VolumeState {
         unsigned *d_tail;       // 4 counters
         void *d_rays;           // spill list
         int cap;                // rays it holds
+        // host output: the tail launch's pixels as (pix, rgb) pairs in
+        // mapped pinned memory, read while the image copy overlaps the tail
+        // launch; 2 + 2 * cap words (word 0: the number of pairs)
+        uint32_t *h_patch;
+        uint32_t *d_patch;      // the same memory seen from the device
+        int patch_cap;
+        cudaStream_t copy_stream;
+        cudaEvent_t tiles_done;
     };
     TailBuf tails[4] = {};
     int n_tails = 0;
@@ -176,8 +184,14 @@ int launch_brick_visibility(const VolumeState *v, const float *const *lut_alpha,
 // Words of visibility bits / floats of MIP bounds of a volume's brick maps.
 inline size_t brick_count(const VolumeState *v) { return (size_t)v->nb[0] * v->nb[1] * v->nb[2]; }
 int finish_output(VolumeState *v, void *out, size_t bytes, int out_on_device, cudaStream_t s);
+// True for page-locked host memory the device can copy to directly.
+bool is_pinned_host(const void *p);
 BrickView brick_view(const VolumeState *v);
 LabelTable label_table(const VolumeState *v);
+// Host-to-device copy of a large pageable buffer on stream s, pipelined
+// through two pinned staging buffers shared by the process (host_stage.cpp);
+// returns once the copy is done.  Below 8 MB: one cudaMemcpyAsync.
+cudaError_t stage_to_device(void *dst, const void *src, size_t bytes, cudaStream_t s);
 
 }  // namespace mk
 

@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(256, 2) k_vr_tail(RayParams P, cudaTextureObje
     __syncthreads();
     const unsigned n = s_n;
     const int tid = threadIdx.x, lane = tid & 31;
+    if (P.patch && blockIdx.x == 0 && tid == 0) P.patch[0] = n;
     const unsigned per = 1;    // rays a warp takes at a time
     const StepVec dv = step_vec(P);
     const float3 L = vr_light(P);
@@ -138,7 +139,12 @@ __global__ void __launch_bounds__(256, 2) k_vr_tail(RayParams P, cudaTextureObje
             float4 sum = R.sum;
             if (sum.x == 0.0f && sum.y == 0.0f && sum.z == 0.0f && sum.w == 0.0f) sum = P.bg;
             const uint32_t rgb = pack_rgb(sum);
-            if (P.rgba) {
+            if (P.patch) {
+                // host output: the image is being copied while this launch
+                // runs; the host applies these pixels after both finish
+                P.patch[2 + 2 * (size_t)(base + lane)] = (uint32_t)R.pix;
+                P.patch[3 + 2 * (size_t)(base + lane)] = rgb;
+            } else if (P.rgba) {
                 reinterpret_cast<uint32_t *>(P.out)[R.pix] = rgb | 0xff000000u;
             } else {
                 uint8_t *o = P.out + (size_t)R.pix * 3;
@@ -236,6 +242,48 @@ static int tail_params(VolumeState &v, RayParams &P, cudaStream_t s) {
     P.spill = static_cast<SpillRay *>(t.d_rays);
     P.spill_cap = t.cap;
     P.tail_trigger = std::max(0, ntiles - K);
+    return MK_OK;
+}
+
+// Host output of a frame with a tail launch: the (pix, rgb) list that the
+// tail launch writes instead of the image, and the stream and event that
+// let the image's copy to the host run while the tail launch does.  Sets
+// *tb to null (and leaves P.patch null: the plain readback) when stream s
+// has no tail buffer or the mapped allocation fails.
+static int tail_patch(VolumeState &v, RayParams &P, cudaStream_t s, VolumeState::TailBuf **tb) {
+    *tb = nullptr;
+    if (!P.tail) return MK_OK;
+    int i = 0;
+    while (i < v.n_tails && v.tails[i].stream != s) ++i;
+    if (i == v.n_tails) return MK_OK;
+    VolumeState::TailBuf &t = v.tails[i];
+    if (!t.copy_stream) {
+        MK_CUDA_TRY(cudaStreamCreateWithFlags(&t.copy_stream, cudaStreamNonBlocking));
+        if (cudaEventCreateWithFlags(&t.tiles_done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            cudaStreamDestroy(t.copy_stream);
+            t.copy_stream = nullptr;
+            return MK_OK;
+        }
+    }
+    if (t.patch_cap < P.spill_cap) {
+        if (t.h_patch) cudaFreeHost(t.h_patch);      // the last frame on s has finished (host output)
+        t.h_patch = t.d_patch = nullptr;
+        t.patch_cap = 0;
+        void *h = nullptr, *d = nullptr;
+        const size_t words = 2 + 2 * (size_t)P.spill_cap;
+        if (cudaHostAlloc(&h, words * sizeof(uint32_t), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+            cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            if (h) cudaFreeHost(h);
+            return MK_OK;
+        }
+        t.h_patch = static_cast<uint32_t *>(h);
+        t.d_patch = static_cast<uint32_t *>(d);
+        t.patch_cap = P.spill_cap;
+    }
+    P.patch = t.d_patch;
+    *tb = &t;
     return MK_OK;
 }
 
@@ -505,6 +553,7 @@ int fill_ray_params(const VolumeState &v, const mk_vr_params *p, RayParams &P) {
     P.spill = nullptr;
     P.spill_cap = 0;
     P.tail_trigger = 0;
+    P.patch = nullptr;
     P.mip_uniform = 0;
     P.mip_ww = 1.0f;
     P.mip_wl = 0.0f;
@@ -547,13 +596,31 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     if (params->render_type == MK_RENDER_MIP) set_mip_window(P, v.present_labels, v.params);
     const bool tail = params->render_type == MK_RENDER_VR && track != kTrackLocal &&
                       !(params->flags & (MK_VR_NO_TAIL | MK_VR_NO_COOP));
+    VolumeState::TailBuf *tb = nullptr;
     if (tail) {
         rc = tail_params(v, P, s);
+        if (rc == MK_OK && !out_on_device) rc = tail_patch(v, P, s, &tb);
         if (rc != MK_OK) return rc;
+    }
+    uint8_t *dst = nullptr;                    // host copy of the image (tb: overlapping the tail launch)
+    if (tb) {
+        if (is_pinned_host(out)) {
+            dst = static_cast<uint8_t *>(out);
+        } else {
+            rc = ensure_pinned_buffer(&v, bytes);
+            if (rc != MK_OK) return rc;
+            dst = static_cast<uint8_t *>(v.h_pinned);
+        }
     }
     launch_raycast<false>(params->render_type, track, P, v.tex_linear, v.tex_mask, label_table(&v),
                           brick_view(&v), order, s);
     MK_CUDA_TRY(cudaGetLastError());
+    if (tb) {
+        // every pixel but the tail launch's is final once the tiles are done
+        MK_CUDA_TRY(cudaEventRecord(tb->tiles_done, s));
+        MK_CUDA_TRY(cudaStreamWaitEvent(tb->copy_stream, tb->tiles_done, 0));
+        MK_CUDA_TRY(cudaMemcpyAsync(dst, P.out, bytes, cudaMemcpyDeviceToHost, tb->copy_stream));
+    }
     if (tail) {
         rc = launch_vr_tail(track, P, v.tex_linear, v.tex_mask, label_table(&v), brick_view(&v), s);
         if (rc != MK_OK) return rc;
@@ -561,7 +628,29 @@ extern "C" int mk_render_vr(mk_volume vol, const mk_vr_params *params, void *out
     rc = note_table_use(v.orders[order_idx].uses, s);
     if (rc == MK_OK) rc = note_table_use(v.fy_tables[fy_idx].uses, s);
     if (rc != MK_OK) return rc;
-    return finish_output(&v, out, bytes, out_on_device, s);
+    if (!tb) return finish_output(&v, out, bytes, out_on_device, s);
+    MK_CUDA_TRY(cudaStreamSynchronize(tb->copy_stream));
+    MK_CUDA_TRY(cudaStreamSynchronize(s));
+    if (dst != out) memcpy(out, dst, bytes);
+    // the tail launch's pixels, from its (pix, rgb) list in mapped memory
+    const volatile uint32_t *pl = tb->h_patch;
+    const uint32_t n_listed = pl[0];
+    const uint32_t n = std::min<uint32_t>(n_listed, (uint32_t)tb->patch_cap);
+    const uint32_t npix = (uint32_t)P.W * (uint32_t)P.H;
+    uint8_t *o = static_cast<uint8_t *>(out);
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t pix = pl[2 + 2 * (size_t)i], rgb = pl[3 + 2 * (size_t)i];
+        if (pix >= npix) continue;
+        if (P.rgba) {
+            const uint32_t w = rgb | 0xff000000u;
+            memcpy(o + (size_t)pix * 4, &w, 4);
+        } else {
+            o[(size_t)pix * 3 + 0] = rgb & 0xff;
+            o[(size_t)pix * 3 + 1] = (rgb >> 8) & 0xff;
+            o[(size_t)pix * 3 + 2] = (rgb >> 16) & 0xff;
+        }
+    }
+    return MK_OK;
 }
 
 __global__ void k_popcount(const uint32_t *__restrict__ bits, size_t nwords, unsigned long long *out) {

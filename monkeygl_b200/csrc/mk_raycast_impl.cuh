@@ -60,6 +60,9 @@ struct RayParams {
     SpillRay *spill;             // rays handed to the tail launch
     int spill_cap;
     int tail_trigger;            // rays still marching spill once this many tiles have finished
+    // tail launch with host output: its pixels go to this (pix, rgb) list
+    // (word 0: the count, pairs from word 2) instead of `out`; null: `out`
+    uint32_t *patch;
     // MIP: 1 when every label present in the mask is visible (alpha > 0) and
     // shares one window (mip_ww > 0, mip_wl); the label fetch is then not
     // needed and the window is applied only to a new raw maximum

@@ -633,7 +633,7 @@ bool brick_rows_fit(int dim_x, int nbx) { return dim_x % kBrick == 0 && nbx <= 2
 
 int upload_linear(const void *host, size_t bytes, void **dptr, cudaStream_t s) {
     MK_CUDA_TRY(cudaMalloc(dptr, bytes));
-    cudaError_t e = cudaMemcpyAsync(*dptr, host, bytes, cudaMemcpyHostToDevice, s);
+    cudaError_t e = stage_to_device(*dptr, host, bytes, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         cudaFree(*dptr);
@@ -736,14 +736,16 @@ int ensure_pinned_buffer(VolumeState *v, size_t bytes) {
 // Copy a finished device output to the caller.  Pinned (or registered)
 // destinations receive the copy directly; pageable ones go through the
 // volume's pinned staging buffer.
+bool is_pinned_host(const void *p) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) == cudaSuccess) return attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    return false;
+}
+
 int finish_output(VolumeState *v, void *out, size_t bytes, int out_on_device, cudaStream_t s) {
     if (out_on_device) return MK_OK;
-    cudaPointerAttributes attr;
-    bool pinned = false;
-    if (cudaPointerGetAttributes(&attr, out) == cudaSuccess)
-        pinned = (attr.type == cudaMemoryTypeHost);
-    else
-        cudaGetLastError();
+    const bool pinned = is_pinned_host(out);
     if (pinned) {
         MK_CUDA_TRY(cudaMemcpyAsync(out, v->d_out, bytes, cudaMemcpyDeviceToHost, s));
         MK_CUDA_TRY(cudaStreamSynchronize(s));
@@ -978,6 +980,9 @@ extern "C" int mk_volume_destroy(mk_volume v) {
     for (int i = 0; i < st.n_tails; ++i) {
         cudaFree(st.tails[i].d_tail);
         cudaFree(st.tails[i].d_rays);
+        if (st.tails[i].h_patch) cudaFreeHost(st.tails[i].h_patch);
+        if (st.tails[i].copy_stream) cudaStreamDestroy(st.tails[i].copy_stream);
+        if (st.tails[i].tiles_done) cudaEventDestroy(st.tails[i].tiles_done);
     }
     for (int i = 0; i < st.n_fy_tables; ++i) {
         cudaFree(st.fy_tables[i].d_fy);
