@@ -202,9 +202,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profile():
+def traffic_from_profile(args):
     """DRAM bytes per frame of the VR launches (tile launch + tail launch)
-    from the committed ncu summary."""
+    from the committed ncu summary of the default workload (body VR, 1024^2,
+    background cap 0.4); None for any other workload, which has no capture."""
+    if (args.workload, args.mode, args.size, args.bg) != ("body", "vr", 1024, 0.4):
+        return None
     p = ROOT / "profiles" / "vr_body_1024_traffic.json"
     if p.exists():
         try:
@@ -384,7 +387,7 @@ def run_mine(args, rank, local, world):
                         "kernel arguments; the RGB image is copied device to host inside the timed region"},
         "frames_crc32": crc,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic_from_profile(),
+                     "frac": round(achieved / peak, 4), "traffic": traffic_from_profile(args),
                      "peak_kind": f"{peak_kind} hbm_gbs (burst copy)",
                      "algorithmic_bytes_per_frame": int(b_alg),
                      "kernel": kernel_desc},

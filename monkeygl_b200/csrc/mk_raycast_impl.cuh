@@ -1118,17 +1118,20 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                 // label fetch is dropped and w is evaluated only when a
                 // sample exceeds the raw maximum so far.  A holds the same
                 // value as in the general loop below after every sample.
-                int k = k0;
+                // The loop below visits the entries k0 .. k_end - 1: those with
+                // accu[k] <= a_stop and accu[k] < limit (the table's last entry
+                // is its first >= limit), the entries the general loop visits.
+                int k_end = accu_lower(P, a_stop);
+                if (P.accu[k_end] <= a_stop) ++k_end;
+                k_end = min(k_end, P.accu_len - 1);
                 float vmax = -INFINITY;
-                while (a < P.limit) {
-                    if (a > a_stop) break;
-                    const float3 pos = ray_pos_at<false>(P, u, v, k, a);
+                for (int k = k0; k < k_end;) {
+                    const float3 pos = ray_pos_fy(P, u, v, P.fy_tab[k]);
                     const int ix = pos.x * P.fdim[0];
                     const int iy = pos.y * P.fdim[1];
                     const int iz = pos.z * P.fdim[2];
                     if (outside_voi(P, ix, iy, iz)) {
-                        k = min(k + 1, P.accu_len - 1);
-                        a = P.accu[k];
+                        ++k;
                         continue;
                     }
                     if (P.skip) {
@@ -1136,8 +1139,7 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                         if (BV.mip_tmax[b] <= A) {
                             const float3 pv = make_float3(pos.x * P.fdim[0], pos.y * P.fdim[1],
                                                           pos.z * P.fdim[2]);
-                            k = min(k + 1 + steps_in_brick(pv, dv, ix, iy, iz), P.accu_len - 1);
-                            a = P.accu[k];
+                            k += 1 + steps_in_brick(pv, dv, ix, iy, iz);
                             continue;
                         }
                     }
@@ -1148,8 +1150,7 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                         temp = (temp - P.mip_wl) / P.mip_ww + 0.5f;
                         if (A < temp) A = temp;
                     }
-                    k = min(k + 1, P.accu_len - 1);
-                    a = P.accu[k];
+                    ++k;
                     // the output saturates at 1.0 (core/kernel.cu:351-358)
                     if (P.skip && A >= 1.0f) break;
                 }
