@@ -126,6 +126,37 @@ def test_rgba_output_and_device_output(small, small_vol):
     assert np.array_equal(dev.cpu().numpy().reshape(rgb.shape), rgb)
 
 
+def test_host_output_paths_agree(labelled):
+    """With host output, the image is copied while the hand-off launch runs
+    and the handed-over pixels are patched in afterwards from the hand-off
+    launch's (pixel, rgb) list.  Pinned and pageable host buffers, RGB and
+    RGBA, on the default and on a caller's stream, must equal the device
+    output of the same frame, which no patch is involved in."""
+    import torch
+    w = labelled
+    v = capi.Volume(w.phantom.volume)
+    v.set_mask(w.phantom.labels)
+    for l, lut in w.luts.items():
+        v.set_transfer_function(l, lut)
+    v.set_label_params(w.label_params)
+    for ang in (0.0, 35.0, 250.0):
+        p = params(w, ang, 0, size=640)
+        dev = torch.empty(p.width * p.height * 3, dtype=torch.uint8, device="cuda")
+        s = torch.cuda.Stream()
+        v.render_vr_device(p, dev.data_ptr(), s.cuda_stream)
+        s.synchronize()
+        want = dev.cpu().numpy().reshape(p.height, p.width, 3)
+        pageable = v.render_vr(p)
+        pinned = torch.empty(p.width * p.height * 3, dtype=torch.uint8, pin_memory=True)
+        v.render_vr(p, out=pinned.numpy().reshape(p.height, p.width, 3))
+        assert np.array_equal(pageable, want), f"pageable {ang}"
+        assert np.array_equal(pinned.numpy().reshape(want.shape), want), f"pinned {ang}"
+        p.pixel_format = capi.PIXEL_RGBA8
+        rgba = v.render_vr(p)
+        assert np.array_equal(rgba[..., :3], want) and (rgba[..., 3] == 255).all(), f"rgba {ang}"
+    v.close()
+
+
 @pytest.mark.parametrize("size", [(77, 33), (333, 45), (1, 1), (2, 511)])
 def test_odd_image_sizes(ref, small, small_vol, size):
     load_ref(ref, small)
