@@ -1261,7 +1261,8 @@ __device__ __forceinline__ void raycast_tile(const RayParams &P, cudaTextureObje
                 if (A <= 0.0f) {
                     sum = P.bg;
                 } else {
-                    const float g = add_dconst(A, MK_DCONST(0.05));
+                    // A + 0.05 in double, rounded to float (core/kernel.cu:460)
+                    const float g = __double2float_rn(__dadd_rn((double)A, 0.05));
                     sum = make_float4(g, g, g, 1.0f);
                 }
             }

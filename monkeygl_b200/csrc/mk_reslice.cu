@@ -8,8 +8,8 @@
 // the trilinear texture scaled by 32768; slabs reduce 2*halfNum+1 samples
 // along the plane normal by max, min or mean.  The coordinate expressions keep
 // MonkeyGL's operation order; its FP64 pieces (the CPR point arithmetic and
-// the slab-mean accumulator) are evaluated with error-free FP32 pairs
-// (mk_math.h).  MK_SAMPLE_NEAREST reads the same voxels through a
+// the slab-mean accumulator) are evaluated in double, operation for
+// operation (FP64 runs at half the FP32 rate on sm_100).  MK_SAMPLE_NEAREST reads the same voxels through a
 // point-filtered texture view.
 //
 // Layout: 256-thread blocks cover 32x8 output tiles so each warp stores one
@@ -34,10 +34,17 @@ __global__ void __launch_bounds__(256) k_plane(PlaneParams P, cudaTextureObject_
     plane_tile<MODE, U8>(P, tex, out, blockIdx.x, blockIdx.y);
 }
 
-// CPR row data: the double point / direction of each row as float pairs.
+// CPR row data: the point and direction of each row, as MonkeyGL passes them.
 struct CprRow {
-    float p_hi[3], p_lo[3], d_hi[3], d_lo[3];
+    double p[3], d[3];
 };
+
+// (float)((p + x * dir) / n) in double, operation for operation as nvcc
+// compiles core/kernel.cu:860-862 (the multiply-add fused; the CPR parity
+// tests compare every pixel with MonkeyGL's kernel).
+__device__ __forceinline__ float cpr_coord_d(double p, double d, int x, float n) {
+    return __double2float_rn(__ddiv_rn(__fma_rn((double)x, d, p), (double)n));
+}
 
 __global__ void __launch_bounds__(256) k_cpr(int W, int H, float3 fdim, int invertZ,
                                              const CprRow *__restrict__ rows,
@@ -50,10 +57,11 @@ __global__ void __launch_bounds__(256) k_cpr(int W, int H, float3 fdim, int inve
     const int x = blockIdx.x * 32 + (threadIdx.x & 31);
     if (x >= W || y >= H) return;
     const CprRow &R = s_rows[ly];
-    const float xf = (float)x;
-    const float fx = cpr_coord(R.p_hi[0], R.p_lo[0], R.d_hi[0], R.d_lo[0], xf, fdim.x);
-    const float fy = cpr_coord(R.p_hi[1], R.p_lo[1], R.d_hi[1], R.d_lo[1], xf, fdim.y);
-    float fz = cpr_coord(R.p_hi[2], R.p_lo[2], R.d_hi[2], R.d_lo[2], xf, fdim.z);
+    const float fx = cpr_coord_d(R.p[0], R.d[0], x, fdim.x);
+    const float fy = cpr_coord_d(R.p[1], R.d[1], x, fdim.y);
+    float fz = cpr_coord_d(R.p[2], R.d[2], x, fdim.z);
+    // "fz = 1.0 - fz" in double, then rounded to float: the float
+    // subtraction rounds the same exact difference once
     if (!invertZ) fz = 1.0f - fz;
     short r;
     if (fx < 0 || fx > 1 || fy < 0 || fy > 1 || fz < 0 || fz > 1) r = -2048;
@@ -219,11 +227,8 @@ extern "C" int mk_render_cpr(mk_volume vol, int width, int height, const double 
     std::vector<CprRow> rows(height);
     for (int y = 0; y < height; ++y) {
         for (int k = 0; k < 3; ++k) {
-            const double p = points[3 * y + k], d = dirs[3 * y + k];
-            rows[y].p_hi[k] = (float)p;
-            rows[y].p_lo[k] = (float)(p - (double)rows[y].p_hi[k]);
-            rows[y].d_hi[k] = (float)d;
-            rows[y].d_lo[k] = (float)(d - (double)rows[y].d_hi[k]);
+            rows[y].p[k] = points[3 * y + k];
+            rows[y].d[k] = dirs[3 * y + k];
         }
     }
     const size_t out_bytes = (size_t)width * height * sizeof(short);
@@ -309,12 +314,9 @@ extern "C" int mk_render_cpr_noalloc(mk_volume vol, int width, int height, const
     CprRow *d_rows = static_cast<CprRow *>(g_noalloc_rows_dev[v.device]);
     for (int y = 0; y < height; ++y) {
         for (int k = 0; k < 3; ++k) {
-            const double p = points[3 * y + k], d = dirs[3 * y + k];
             CprRow &r = g_noalloc_rows_host[y];
-            r.p_hi[k] = (float)p;
-            r.p_lo[k] = (float)(p - (double)r.p_hi[k]);
-            r.d_hi[k] = (float)d;
-            r.d_lo[k] = (float)(d - (double)r.d_hi[k]);
+            r.p[k] = points[3 * y + k];
+            r.d[k] = dirs[3 * y + k];
         }
     }
     // pageable source: the call returns once the rows are staged, so the host

@@ -28,7 +28,7 @@ template <int MODE>
 __device__ __forceinline__ short reslice_pixel(const PlaneParams &P, cudaTextureObject_t tex, int x,
                                                int y) {
     short acc = (MODE == MK_MPR_MIP) ? (short)-32768 : (short)32767;
-    fsum sum = {0.0f, 0.0f};
+    double sum = 0.0;          // MonkeyGL's double accumulator (core/kernel.cu:773)
     // The contraction of MonkeyGL's sums pt + x*ps*h + y*ps*v into fused
     // multiply-adds is spelled out, left to right: of the fused and unfused
     // orders, this one reproduces MonkeyGL's kernel pixel for pixel, and
@@ -47,14 +47,19 @@ __device__ __forceinline__ short reslice_pixel(const PlaneParams &P, cudaTexture
         if (!P.invertZ) fz = 1.0f - fz;
         const bool inside = fx >= 0 && fx <= 1 && fy >= 0 && fy <= 1 && fz >= 0 && fz <= 1;
         if (MODE == MK_MPR_AVERAGE) {
-            fsum_add(sum, inside ? 32768 * tex3D<float>(tex, fx, fy, fz) : -32768.0f);
+            sum = __dadd_rn(sum, (double)(inside ? 32768 * tex3D<float>(tex, fx, fy, fz) : -32768.0f));
         } else {
             const short val = inside ? f2s_sat(32768 * tex3D<float>(tex, fx, fy, fz)) : (short)-32768;
             if (MODE == MK_MPR_MIP) acc = acc > val ? acc : val;
             else acc = acc < val ? acc : val;
         }
     }
-    if (MODE == MK_MPR_AVERAGE) return fsum_div_to_short(sum, 2 * P.halfNum + 1);
+    if (MODE == MK_MPR_AVERAGE) {
+        // fSum / (2 * halfNum + 1) in double, converted to short (truncated,
+        // saturated as the conversion instruction does)
+        const double q = __ddiv_rn(sum, (double)(2 * P.halfNum + 1));
+        return (short)min(max(__double2int_rz(q), -32768), 32767);
+    }
     return acc;
 }
 
