@@ -180,6 +180,19 @@ int mk_volume_brick_maps(mk_volume vol, int *nb, int16_t *minmax, uint32_t *labe
 int mk_volume_set_mask(mk_volume vol, const uint8_t *labels);
 
 /*
+ * Incremental form of mk_volume_set_mask for a mask that changed only inside
+ * box = {x0, y0, z0, x1, y1, z1} (voxels x0 <= x < x1 etc.): `labels` is the
+ * whole updated uint8 label volume (same dims and layout), of which only the
+ * box, widened to whole 8^3 bricks, is copied to the device and re-bricked.
+ * MonkeyGL re-uploads the whole mask on every object added or updated
+ * (DataManager.cpp:280-335, CuDataManager.cu:75-120).  The volume must have
+ * a mask already (MK_ERR_INVALID_ARGUMENT otherwise); labels that the update
+ * removed everywhere stay listed as present (the per-ray state they size is
+ * then larger than needed, never smaller).
+ */
+int mk_volume_update_mask(mk_volume vol, const uint8_t *labels, const int box[6]);
+
+/*
  * Set the RGBA lookup table of one label: `n_entries` float4 (r,g,b,a) in
  * [0,1], filtered linearly over t in [0,1] with entry centres at (i+0.5)/n.
  * Replaces cu_setTransferFunc (core/CuDataManager.cu:122-163).  A label with

@@ -126,6 +126,7 @@ _SIGS = {
     "mk_volume_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     "mk_volume_dims": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "mk_volume_set_mask": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "mk_volume_update_mask": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "mk_volume_brick_maps": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.c_void_p, C.c_void_p,
                                        C.POINTER(C.c_uint64)]),
     "mk_volume_set_transfer_function": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
@@ -252,6 +253,15 @@ class Volume:
         if m.shape != self.dims[::-1]:
             raise ValueError("label volume shape differs from the voxels")
         _check(lib().mk_volume_set_mask(self.handle, _ptr(m)), "mk_volume_set_mask")
+
+    def update_mask(self, labels: np.ndarray, box):
+        """Re-upload only box = (x0, y0, z0, x1, y1, z1) of the updated label
+        volume `labels` (mk_volume_update_mask)."""
+        m = np.ascontiguousarray(labels, dtype=np.uint8)
+        if m.shape != self.dims[::-1]:
+            raise ValueError("label volume shape differs from the voxels")
+        b = (C.c_int * 6)(*[int(v) for v in box])
+        _check(lib().mk_volume_update_mask(self.handle, _ptr(m), b), "mk_volume_update_mask")
 
     def brick_maps(self):
         """(minmax (nbz, nby, nbx, 2) int16, labels (nbz, nby, nbx, 3) uint32,

@@ -371,8 +371,14 @@ unsigned char Engine::AddNewObjectMask(std::shared_ptr<unsigned char> data, int 
     }
     unsigned char *m = mask_.get();
     const unsigned char *p = data.get();
-    for (size_t i = 0; i < n; ++i)
-        if (p[i] > 0) m[i] = label;
+    size_t i = 0;
+    for (int z = 0; z < d; ++z)
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x, ++i)
+                if (p[i] > 0 && m[i] != label) {
+                    m[i] = label;
+                    GrowMaskBox(x, y, z);
+                }
     objects_[label] = objects_[(unsigned char)activeLabel_];
     activeLabel_ = label;
     maskDirty_ = true;
@@ -386,12 +392,29 @@ bool Engine::UpdateObjectMask(std::shared_ptr<unsigned char> data, int w, int h,
     const size_t n = (size_t)w * h * d;
     unsigned char *m = mask_.get();
     const unsigned char *p = data.get();
-    for (size_t i = 0; i < n; ++i) {
-        if (p[i] > 0) m[i] = label;
-        else if (p[i] == 0 && m[i] == label) m[i] = 0;
-    }
+    size_t i = 0;
+    for (int z = 0; z < d; ++z)
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x, ++i) {
+                const unsigned char nv = p[i] > 0 ? label : (m[i] == label ? 0 : m[i]);
+                if (nv != m[i]) {
+                    m[i] = nv;
+                    GrowMaskBox(x, y, z);
+                }
+            }
+    (void)n;
     maskDirty_ = true;
     return true;
+}
+
+void Engine::GrowMaskBox(int x, int y, int z) {
+    int *b = maskBox_;
+    if (b[0] >= b[3]) {   // empty
+        b[0] = x, b[1] = y, b[2] = z, b[3] = x + 1, b[4] = y + 1, b[5] = z + 1;
+        return;
+    }
+    b[0] = std::min(b[0], x), b[1] = std::min(b[1], y), b[2] = std::min(b[2], z);
+    b[3] = std::max(b[3], x + 1), b[4] = std::max(b[4], y + 1), b[5] = std::max(b[5], z + 1);
 }
 
 // ---- transfer functions and windows (DataManager.cpp:337-611) -------------
@@ -1152,11 +1175,21 @@ bool Engine::SyncDevice() {
         }
         volumeDirty_ = false;
         maskDirty_ = true;
+        maskOnDevice_ = false;      // a new device volume: the whole mask goes up
         tfDirty_ = true;
         tableDirty_ = true;
     }
     if (maskDirty_) {
-        if (mk_volume_set_mask(dev_, mask_ ? mask_.get() : nullptr) != MK_OK) return false;
+        // a mask already on the device is updated in the box that changed
+        // (MonkeyGL re-uploads the whole mask, CuDataManager.cu:75-120)
+        if (maskOnDevice_ && mask_) {
+            if (maskBox_[0] < maskBox_[3] && mk_volume_update_mask(dev_, mask_.get(), maskBox_) != MK_OK)
+                return false;
+        } else if (mk_volume_set_mask(dev_, mask_ ? mask_.get() : nullptr) != MK_OK) {
+            return false;
+        }
+        maskOnDevice_ = mask_ != nullptr;
+        maskBox_[0] = maskBox_[3] = 0;
         maskDirty_ = false;
     }
     if (tfDirty_) {

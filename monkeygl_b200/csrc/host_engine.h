@@ -227,6 +227,11 @@ private:
     // device
     mk_volume dev_ = nullptr;
     bool tfDirty_ = true, tableDirty_ = true, maskDirty_ = false, volumeDirty_ = false;
+    // the device holds the mask as of the last upload; voxels changed since
+    // lie in maskBox_ (x0, y0, z0, x1, y1, z1, exclusive; empty when x0 >= x1)
+    bool maskOnDevice_ = false;
+    int maskBox_[6] = {0, 0, 0, 0, 0, 0};
+    void GrowMaskBox(int x, int y, int z);
 };
 
 }  // namespace detail

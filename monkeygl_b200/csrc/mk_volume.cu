@@ -112,6 +112,50 @@ __global__ void __launch_bounds__(256) k_brick_labels(const unsigned char *__res
     if (lane < 3) out[3 * (size_t)b + lane] = lane == 0 ? m0 : (lane == 1 ? m1 : m2);
 }
 
+// Label sets of the bricks of a brick-aligned sub-box (one warp per brick,
+// as k_brick_labels): `lab` holds the sub-box (ex x ey x ez voxels, x
+// fastest) whose first voxel is brick (bx0, by0, bz0) of the volume; the
+// sets go to the volume's brick numbering and are OR-ed into present[0..2].
+__global__ void __launch_bounds__(256) k_brick_labels_box(const unsigned char *__restrict__ lab, int ex, int ey,
+                                                          int ez, int bx0, int by0, int bz0, int nbx, int nby,
+                                                          uint32_t *out, uint32_t *present) {
+    const int snbx = (ex + kBrick - 1) / kBrick, snby = (ey + kBrick - 1) / kBrick;
+    const int snbz = (ez + kBrick - 1) / kBrick;
+    const int b = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (b >= snbx * snby * snbz) return;
+    const int lane = threadIdx.x & 31;
+    const int sbx = b % snbx, sby = (b / snbx) % snby, sbz = b / (snbx * snby);
+    const int x0 = sbx * kBrick, x1 = min(x0 + kBrick, ex) - 1;
+    const int y0 = sby * kBrick, y1 = min(y0 + kBrick, ey) - 1;
+    const int z0 = sbz * kBrick, z1 = min(z0 + kBrick, ez) - 1;
+    const int x = x0 + (lane & 7), row = lane >> 3;
+    uint32_t m0 = 0, m1 = 0, m2 = 0;
+    if (x <= x1 && y0 + row <= y1) {
+        const size_t plane = (size_t)ey * ex, step = 4 * (size_t)ex;
+        const int nrows = (y1 - y0 - row) / 4 + 1;   // 1 or 2
+        const unsigned char *q0 = lab + (size_t)z0 * plane + (size_t)(y0 + row) * ex + x;
+        for (int z = z0; z <= z1; ++z, q0 += plane) {
+            const unsigned char *q = q0;
+            for (int r = 0; r < nrows; ++r, q += step) {
+                int l = __ldg(q);
+                if (l > 64) l = 64;
+                if (l < 32) m0 |= 1u << l;
+                else if (l < 64) m1 |= 1u << (l - 32);
+                else m2 |= 1u;
+            }
+        }
+    }
+    m0 = __reduce_or_sync(0xffffffffu, m0);
+    m1 = __reduce_or_sync(0xffffffffu, m1);
+    m2 = __reduce_or_sync(0xffffffffu, m2);
+    const size_t gb = ((size_t)(bz0 + sbz) * nby + (by0 + sby)) * nbx + (bx0 + sbx);
+    if (lane < 3) {
+        const uint32_t w = lane == 0 ? m0 : (lane == 1 ? m1 : m2);
+        out[3 * gb + lane] = w;
+        if (w) atomicOr(&present[lane], w);
+    }
+}
+
 // The same two maps by rows of vectors, for volumes whose rows split into
 // whole bricks (dim_x a multiple of 8, at most 256 bricks across): thread t
 // of a block owns x-brick t of one brick row (blockIdx.x) for a run of
@@ -1149,6 +1193,88 @@ extern "C" int mk_volume_set_mask(mk_volume v, const uint8_t *labels) {
     }
     st.present_labels[0] = pres[0];
     st.present_labels[1] = pres[1];
+    return MK_OK;
+}
+
+extern "C" int mk_volume_update_mask(mk_volume v, const uint8_t *labels, const int box[6]) {
+    if (!v || !labels || !box) {
+        set_last_error("mk_volume_update_mask: null argument");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    VolumeState &st = v->st;
+    if (!st.mask_array) {
+        set_last_error("mk_volume_update_mask: the volume has no mask (use mk_volume_set_mask)");
+        return MK_ERR_INVALID_ARGUMENT;
+    }
+    const int dx = st.dims[0], dy = st.dims[1], dz = st.dims[2];
+    const int lo[3] = {box[0], box[1], box[2]}, hi[3] = {box[3], box[4], box[5]};
+    const int dim[3] = {dx, dy, dz};
+    for (int k = 0; k < 3; ++k) {
+        if (lo[k] < 0 || hi[k] > dim[k] || lo[k] >= hi[k]) {
+            set_last_error("mk_volume_update_mask: box outside the volume or empty");
+            return MK_ERR_INVALID_ARGUMENT;
+        }
+    }
+    // widen to whole bricks (clamped to the volume): a brick's label set
+    // depends on its own voxels only
+    int b0[3], e[3];
+    for (int k = 0; k < 3; ++k) {
+        b0[k] = lo[k] & ~(kBrick - 1);
+        e[k] = std::min((hi[k] + kBrick - 1) & ~(kBrick - 1), dim[k]) - b0[k];
+    }
+    DeviceGuard guard(st.device);
+    // the array is written in place: renders of this volume on any stream
+    // must have finished reading it
+    MK_CUDA_TRY(cudaDeviceSynchronize());
+    const size_t sub = (size_t)e[0] * e[1] * e[2];
+    unsigned char *d_sub = nullptr;
+    uint32_t *d_present = nullptr;
+    if (cudaMalloc(&d_sub, sub) != cudaSuccess || cudaMalloc(&d_present, 3 * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(d_sub);
+        set_last_error("mk_volume_update_mask: allocation failed");
+        return MK_ERR_OUT_OF_MEMORY;
+    }
+    uint32_t h_present[3] = {0, 0, 0};
+    cudaError_t err = cudaMemsetAsync(d_present, 0, 3 * sizeof(uint32_t), st.stream);
+    // host box -> linear device box -> the mask array at the box's place
+    cudaMemcpy3DParms hp;
+    memset(&hp, 0, sizeof(hp));
+    hp.srcPtr = make_cudaPitchedPtr(const_cast<uint8_t *>(labels), dx, dx, dy);
+    hp.srcPos = make_cudaPos(b0[0], b0[1], b0[2]);
+    hp.dstPtr = make_cudaPitchedPtr(d_sub, e[0], e[0], e[1]);
+    hp.extent = make_cudaExtent(e[0], e[1], e[2]);
+    hp.kind = cudaMemcpyHostToDevice;
+    if (err == cudaSuccess) err = cudaMemcpy3DAsync(&hp, st.stream);
+    cudaMemcpy3DParms ap;
+    memset(&ap, 0, sizeof(ap));
+    ap.srcPtr = make_cudaPitchedPtr(d_sub, e[0], e[0], e[1]);
+    ap.dstArray = st.mask_array;
+    ap.dstPos = make_cudaPos(b0[0], b0[1], b0[2]);
+    ap.extent = make_cudaExtent(e[0], e[1], e[2]);
+    ap.kind = cudaMemcpyDeviceToDevice;
+    if (err == cudaSuccess) err = cudaMemcpy3DAsync(&ap, st.stream);
+    if (err == cudaSuccess) {
+        const int nsub = ((e[0] + kBrick - 1) / kBrick) * ((e[1] + kBrick - 1) / kBrick) *
+                         ((e[2] + kBrick - 1) / kBrick);
+        k_brick_labels_box<<<(unsigned)((nsub + 7) / 8), 256, 0, st.stream>>>(
+            d_sub, e[0], e[1], e[2], b0[0] / kBrick, b0[1] / kBrick, b0[2] / kBrick, st.nb[0], st.nb[1],
+            st.d_labels, d_present);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(h_present, d_present, sizeof(h_present), cudaMemcpyDeviceToHost, st.stream);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(st.stream);
+    cudaFree(d_sub);
+    cudaFree(d_present);
+    if (err != cudaSuccess) {
+        set_last_error(std::string("mk_volume_update_mask: ") + cudaGetErrorString(err));
+        return MK_ERR_CUDA;
+    }
+    // labels can only be added to the set here (see the header)
+    st.present_labels[0] |= (uint64_t)h_present[0] | ((uint64_t)h_present[1] << 32);
+    st.present_labels[1] |= h_present[2] & 1u;
+    st.maps_dirty = true;
     return MK_OK;
 }
 

@@ -157,6 +157,12 @@ def run_both(p, ops, masks=None):
                                pm.RGBA(*rgba))
         elif k == "clear_annotations":
             L.mkrh_remove_annotations(h); mine.RemoveAllAnnotations()
+        elif k == "add_mask":
+            a = L.mkrh_add_mask(h, ptr(op[1]), X, Y, Z)
+            b = mine.AddNewObjectMaskArray(op[1].swapaxes(2, 0))
+            assert a == b
+        elif k == "render_mine":
+            mine.GetVRImage()       # the mask goes to the device here; later masks update it in place
         else:
             raise ValueError(k)
     return ref, mine
@@ -265,6 +271,26 @@ def test_multilabel_vr_through_the_api(phantom):
            ("rotate", 60, 0), ("vr_size", 640, 480)]
     ref, mine = run_both(phantom, ops, masks)
     assert_vr_equal(mine.GetVRImage(), ref_vr(ref), "multi-label VR")
+
+
+def test_incremental_masks_through_the_api(phantom):
+    """Masks added after the first render reach the device as an update of
+    the box they change (mk_volume_update_mask), MonkeyGL re-uploads its
+    whole mask; the images must agree after every addition."""
+    labels = phantom.labels
+    X, Y, Z = phantom.dims
+    first = (labels == 1).astype(np.uint8)
+    small = np.zeros_like(first)
+    small[40:52, 30:61, 70:77] = 1                  # a box that is not brick-aligned
+    edge = np.zeros_like(first)
+    edge[Z - 5:, Y - 9:, :17] = 1                   # touching the volume's far faces
+    ops = [("tf", TF4, {}, 0), ("tf", {0: (1, 0, 0, 0.1), 99: (1, 1, 0, 0.9)}, {}, 1),
+           ("wwwl", 1700, 650, 0), ("wwwl", 1200, 400, 1), ("alpha", 0.4, 0), ("rotate", 35, 15),
+           ("render_mine",), ("add_mask", (labels == 2).astype(np.uint8)), ("render_mine",),
+           ("add_mask", small), ("render_mine",), ("add_mask", edge),
+           ("tf", {0: (0, 1, 0, 0.0), 50: (0, 1, 1, 0.6), 99: (0, 0, 1, 1)}, {}, 4), ("alpha", 0.8, 3)]
+    ref, mine = run_both(phantom, ops, [first])
+    assert_vr_equal(mine.GetVRImage(), ref_vr(ref), "VR after incremental mask updates")
 
 
 def test_planes_through_the_api(phantom):

@@ -98,3 +98,52 @@ def test_brick_maps_shapes(dims):
     lab[:, : Y // 2] = 0
     check_maps(vox, lab, f"{dims}")
     check_maps(vox, None, f"{dims} no labels")
+
+
+def test_incremental_mask_update_matches_full_upload():
+    """mk_volume_update_mask re-uploads and re-bricks only a box: the brick
+    label sets must equal numpy's on the final labels, and every render must
+    equal a volume given the final labels in one mk_volume_set_mask."""
+    from monkeygl_b200.camera import view_camera
+    rng = np.random.default_rng(77)
+    X, Y, Z = 100, 90, 70                 # rows not whole bricks: the box kernels see partial bricks
+    vox = rng.integers(-1000, 2000, (Z, Y, X), dtype=np.int32).astype(np.int16)
+    lab = np.zeros((Z, Y, X), np.uint8)
+    lab[10:40, 20:60, 30:80] = 1
+    a = capi.Volume(vox)
+    a.set_mask(lab)
+    lut = np.zeros((256, 4), np.float32)
+    lut[:, 0] = np.linspace(0, 1, 256)
+    lut[:, 1] = 0.5
+    lut[:, 2] = np.linspace(1, 0, 256)
+    lut[:, 3] = np.linspace(0, 0.3, 256)
+    lp = np.zeros((65, 3), np.float32)
+    lp[:, 1] = 1.0
+    for l in range(4):
+        a.set_transfer_function(l, lut)
+        lp[l] = (0.9 if l else 0.5, 1700.0, 650.0)
+    a.set_label_params(lp)
+    p = capi.vr_params(160, 120, 0, view_camera(25.0), (X, Y, Z), (1, 1, 1))
+    a.render_vr(p)                        # maps built for the first mask
+    boxes = [(33, 17, 5, 47, 29, 21, 2), (0, 0, 0, 8, 8, 8, 3), (91, 83, 61, 100, 90, 70, 2), (5, 3, 50, 97, 88, 69, 0)]
+    for x0, y0, z0, x1, y1, z1, val in boxes:
+        lab[z0:z1, y0:y1, x0:x1] = val
+        a.update_mask(lab, (x0, y0, z0, x1, y1, z1))
+        _, words, present = a.brick_maps()
+        want, _ = numpy_label_sets(lab)
+        assert np.array_equal(words, want), f"label sets after box {(x0, y0, z0, x1, y1, z1)}"
+        assert present[val] and present[0]
+        b = capi.Volume(vox)
+        b.set_mask(lab)
+        for l in range(4):
+            b.set_transfer_function(l, lut)
+        b.set_label_params(lp)
+        for ang in (25.0, 140.0):
+            q = capi.vr_params(160, 120, 0, view_camera(ang), (X, Y, Z), (1, 1, 1))
+            assert np.array_equal(a.render_vr(q), b.render_vr(q)), f"VR {ang} after box {(x0, y0, z0)}"
+            q = capi.vr_params(160, 120, 1, view_camera(ang), (X, Y, Z), (1, 1, 1))
+            assert np.array_equal(a.render_vr(q), b.render_vr(q)), f"MIP {ang} after box {(x0, y0, z0)}"
+        b.close()
+    with pytest.raises(capi.MonkeyGLError):
+        a.update_mask(lab, (0, 0, 0, X + 1, 4, 4))
+    a.close()
