@@ -156,18 +156,11 @@ __global__ void __launch_bounds__(256) k_brick_labels_box(const unsigned char *_
     }
 }
 
-// The same two maps by rows of vectors, for volumes whose rows split into
-// whole bricks (dim_x a multiple of 8, at most 256 bricks across): thread t
-// of a block owns x-brick t of one brick row (blockIdx.x) for a run of
-// kZRun z-bricks (blockIdx.y), reads each voxel row of its brick as one
-// 16-byte vector (8 int16) and keeps packed min/max with the paired-int16
-// SIMD instructions.  The x halo of a row -- the last voxel of the brick to
-// the left, the first of the brick to the right -- comes from the
-// neighbouring lanes by shuffle (lanes 0 and 31 read it).  Slices are read
-// once per run: the slice below a brick and its first slice are both
-// carried in registers from the previous brick.  Every load of a warp is a
-// contiguous 512-byte row segment; the y halo rows are the neighbouring
-// brick rows' own rows, read again from L2.
+// Packed int16 min/max of 8 voxels of a row (uint4 of paired int16, SIMD
+// vmins2/vmaxs2) plus the min/max of the row's two x-halo voxels, for the
+// staged min/max kernel below; the label-set row kernel shares the brick-row
+// decomposition: a block owns one brick row (blockIdx.x) for a run of kZRun
+// z-bricks (blockIdx.y), thread t owns x-brick t.
 constexpr int kZRun = 4;
 
 struct Mm8 {
@@ -195,77 +188,12 @@ __device__ __forceinline__ void mm8_merge(Mm8 &a, const Mm8 &b) {
     a.hhi = max(a.hhi, b.hhi);
 }
 
-// Min/max of slice z over the brick's x range grown by one voxel and the
-// ten rows yrow[0..9] (the brick's rows grown by one, clamped).  Called by
-// every lane of the warp (the shuffles need all 32).
-__device__ __forceinline__ Mm8 mm8_slice(const short *__restrict__ vox, size_t zoff, int dx, const int *yrow,
-                                         int x0, int lane, bool left, bool right) {
-    Mm8 m;
-    mm8_init(m);
-    uint4 v[10];
-#pragma unroll
-    for (int r = 0; r < 10; ++r)
-        v[r] = __ldg(reinterpret_cast<const uint4 *>(vox + zoff + (size_t)yrow[r] * dx + x0));
-#pragma unroll
-    for (int r = 0; r < 10; ++r) {
-        m.lo.x = __vmins2(m.lo.x, v[r].x);
-        m.lo.y = __vmins2(m.lo.y, v[r].y);
-        m.lo.z = __vmins2(m.lo.z, v[r].z);
-        m.lo.w = __vmins2(m.lo.w, v[r].w);
-        m.hi.x = __vmaxs2(m.hi.x, v[r].x);
-        m.hi.y = __vmaxs2(m.hi.y, v[r].y);
-        m.hi.z = __vmaxs2(m.hi.z, v[r].z);
-        m.hi.w = __vmaxs2(m.hi.w, v[r].w);
-        int l = (short)(__shfl_up_sync(0xffffffffu, v[r].w, 1) >> 16);     // voxel x0 - 1
-        int h = (short)(__shfl_down_sync(0xffffffffu, v[r].x, 1) & 0xffffu); // voxel x0 + 8
-        if (lane == 0 && left) l = __ldg(vox + zoff + (size_t)yrow[r] * dx + x0 - 1);
-        if (lane == 31 && right) h = __ldg(vox + zoff + (size_t)yrow[r] * dx + x0 + 8);
-        if (!left) l = (short)(v[r].x & 0xffffu);
-        if (!right) h = (short)(v[r].w >> 16);
-        m.hlo = min(m.hlo, min(l, h));
-        m.hhi = max(m.hhi, max(l, h));
-    }
-    return m;
-}
-
 __device__ __forceinline__ short2 mm8_result(const Mm8 &m) {
     uint32_t lo = __vmins2(__vmins2(m.lo.x, m.lo.y), __vmins2(m.lo.z, m.lo.w));
     uint32_t hi = __vmaxs2(__vmaxs2(m.hi.x, m.hi.y), __vmaxs2(m.hi.z, m.hi.w));
     const int l = min(min((int)(short)(lo & 0xffffu), (int)(short)(lo >> 16)), m.hlo);
     const int h = max(max((int)(short)(hi & 0xffffu), (int)(short)(hi >> 16)), m.hhi);
     return make_short2((short)l, (short)h);
-}
-
-__global__ void __launch_bounds__(256) k_brick_minmax_rows(const short *__restrict__ vox, int dx, int dy, int dz,
-                                                            int nbx, int nby, int nbz, short2 *out) {
-    const int lane = threadIdx.x & 31;
-    const int bx = min((int)threadIdx.x, nbx - 1);   // lanes past the last brick repeat it and store nothing
-    const bool owner = (int)threadIdx.x < nbx;
-    const int by = blockIdx.x;
-    const int bz0 = blockIdx.y * kZRun, bz1 = min(bz0 + kZRun, nbz);
-    const int x0 = bx * kBrick;
-    const bool left = bx > 0, right = bx + 1 < nbx;
-    int yrow[10];
-#pragma unroll
-    for (int r = 0; r < 10; ++r) yrow[r] = min(max(by * kBrick - 1 + r, 0), dy - 1);
-    const size_t plane = (size_t)dx * dy;
-    const int za = max(bz0 * kBrick - 1, 0), zb = min(bz1 * kBrick, dz - 1);
-    Mm8 acc, prev;
-    mm8_init(acc);
-    mm8_init(prev);
-    int cur = bz0;
-    for (int z = za; z <= zb; ++z) {
-        const Mm8 S = mm8_slice(vox, (size_t)z * plane, dx, yrow, x0, lane, left, right);
-        mm8_merge(acc, S);
-        if ((z >> kBrickShift) > cur) {       // z = 8 (cur + 1): the slice above brick cur
-            if (owner) out[((size_t)cur * nby + by) * nbx + bx] = mm8_result(acc);
-            if (++cur >= bz1) break;
-            acc = prev;                       // the slice below brick cur, then its first slice
-            mm8_merge(acc, S);
-        }
-        prev = S;
-    }
-    if (cur < bz1 && owner) out[((size_t)cur * nby + by) * nbx + bx] = mm8_result(acc);
 }
 
 // Label sets by rows: thread t owns x-brick t of one brick row for kZRun
@@ -345,8 +273,8 @@ __global__ void __launch_bounds__(256) k_brick_labels_rows(const unsigned char *
 // row segment and both halo voxels from shared memory, and the stage is
 // refilled with the slice kStages ahead once all threads have read it.  The
 // loads of a block so run ahead of its arithmetic by kStages slices whatever
-// the register count (the register-staged row kernels above wait on their
-// loads: ncu shows long-scoreboard stalls).  Waits are bounded: a stage that
+// the register count (kernels that load rows into registers wait on those
+// loads: ncu showed long-scoreboard stalls).  Waits are bounded: a stage that
 // does not complete within kStageWaitNs sets *err, and the block waits
 // (bounded again) for its own copies before it returns.
 constexpr int kStages = 4;
@@ -471,7 +399,7 @@ __global__ void __launch_bounds__(256) k_brick_minmax_staged(const short *__rest
             S.hi.y = __vmaxs2(S.hi.y, v.y);
             S.hi.z = __vmaxs2(S.hi.z, v.z);
             S.hi.w = __vmaxs2(S.hi.w, v.w);
-            // x halo from the neighbouring lanes, as mm8_slice (lanes 0 and 31 read it)
+            // x halo from the neighbouring lanes (lanes 0 and 31 read it from the row)
             int l = (short)(__shfl_up_sync(0xffffffffu, v.w, 1) >> 16);
             int h = (short)(__shfl_down_sync(0xffffffffu, v.x, 1) & 0xffffu);
             if (lane == 0 && left) l = row[x0 - 1];
@@ -936,10 +864,6 @@ extern "C" int mk_volume_create(mk_volume *out, const int16_t *voxels, int dim_x
             k_brick_minmax_staged<<<grid, (st.nb[0] + 31) & ~31, smem, st.stream>>>(
                 (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], st.nb[2], st.d_minmax,
                 reinterpret_cast<unsigned *>(st.d_counter));
-        } else if (brick_rows_fit(dim_x, st.nb[0])) {
-            const dim3 grid(st.nb[1], (st.nb[2] + kZRun - 1) / kZRun);
-            k_brick_minmax_rows<<<grid, (st.nb[0] + 31) & ~31, 0, st.stream>>>(
-                (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], st.nb[2], st.d_minmax);
         } else {
             k_brick_minmax<<<(unsigned)((nbricks + 7) / 8), 256, 0, st.stream>>>(
                 (const short *)d_lin, dim_x, dim_y, dim_z, st.nb[0], st.nb[1], (int)nbricks, st.d_minmax);
