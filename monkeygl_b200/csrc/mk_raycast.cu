@@ -54,9 +54,13 @@ namespace mk {
 // (index by * tiles_x + bx): the launch takes tiles centre first, where the
 // projected volume -- and the longest rays -- usually are, so they start in
 // the first wave instead of forming the tail of the launch.  Register
-// budgets: VR 64 (four blocks per SM), MIP and surface 40 (six).
+// budgets, measured on 1024^2 frames: VR 48 (five blocks per SM; four and
+// six were slower on the body and cardiac frames), MIP and surface 40 (six;
+// eight, at 32 registers, was slower).
+constexpr int kVrBlocksPerSm = 5;
+constexpr int kRayBlocksPerSm = 6;
 template <int MODE, int TRACK, bool COUNT>
-__global__ void __launch_bounds__(256, MODE == kModeVR ? 4 : 6) k_raycast(RayParams P, cudaTextureObject_t vol,
+__global__ void __launch_bounds__(256, MODE == kModeVR ? kVrBlocksPerSm : kRayBlocksPerSm) k_raycast(RayParams P, cudaTextureObject_t vol,
                                                  cudaTextureObject_t mask, LabelTable LT,
                                                  BrickView BV, const int *__restrict__ order) {
     __shared__ LabelSmem S;
