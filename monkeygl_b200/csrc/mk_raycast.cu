@@ -59,6 +59,9 @@ namespace mk {
 // eight, at 32 registers, was slower).
 constexpr int kVrBlocksPerSm = 5;
 constexpr int kRayBlocksPerSm = 6;
+// The hand-off launch: two blocks per SM (up to 128 registers); three and
+// four (80 and 64 registers) were slower on the body frame.
+constexpr int kTailBlocksPerSm = 2;
 template <int MODE, int TRACK, bool COUNT>
 __global__ void __launch_bounds__(256, MODE == kModeVR ? kVrBlocksPerSm : kRayBlocksPerSm) k_raycast(RayParams P, cudaTextureObject_t vol,
                                                  cudaTextureObject_t mask, LabelTable LT,
@@ -91,7 +94,7 @@ __global__ void __launch_bounds__(256, MODE == kModeVR ? kVrBlocksPerSm : kRayBl
 // +1.1%, cardiac +1.9%), writes their pixels, and resets the frame's tail
 // counters for the next frame.
 template <int TRACK>
-__global__ void __launch_bounds__(256, 2) k_vr_tail(RayParams P, cudaTextureObject_t vol, cudaTextureObject_t mask,
+__global__ void __launch_bounds__(256, kTailBlocksPerSm) k_vr_tail(RayParams P, cudaTextureObject_t vol, cudaTextureObject_t mask,
                                                  LabelTable LT, BrickView BV) {
     __shared__ LabelSmem S;
     __shared__ float s_acc[TRACK == kTrackShared ? kMaxTrackedLabels : 1][256];
