@@ -338,10 +338,12 @@ int mk_dvr_backward(const mk_dvr_params *views, int nviews, const float *volume,
  *   - The per-row table lives in a fixed device array of 4096 rows (192 KiB)
  *     that every GPU loading this library holds until the process exits;
  *     height > 4096 is rejected with MK_ERR_INVALID_ARGUMENT and a message.
- *   - The first call on a device looks up that array's device address; make
- *     that first call before any stream capture.  The address is kept until
- *     the process exits, so the call is not for use on a device after a
- *     cudaDeviceReset in the same process.
+ *   - The first call on a device looks up that array's device address.  The
+ *     address is kept until the process exits, so the call is not for use on
+ *     a device after a cudaDeviceReset in the same process.
+ *   - The rows reach the device by a copy from one process-wide host table,
+ *     so the call must not be recorded under stream capture: a replayed
+ *     graph would copy whatever rows the latest call left there.
  *   - The call is asynchronous on `stream` (NULL = the volume's stream).
  *     Every call shares the one array (each call overwrites the rows it
  *     uses; nothing needs to start at zero), so calls that overlap on the
