@@ -79,6 +79,9 @@ def test_entry_points_reject_null_handles():
     assert L.mk_render_plane(None, C.byref(capi.PlaneParams()), C.c_void_p(buf.ctypes.data), 0, None) == 1
     assert L.mk_render_cpr(None, 4, 4, None, None, 0, None, 0, None) == 1
     assert L.mk_volume_set_mask(None, None) == 1
+    box = (C.c_int * 6)(0, 0, 0, 1, 1, 1)
+    assert L.mk_volume_update_mask(None, C.c_void_p(buf.ctypes.data), box) == 1
+    assert L.mk_volume_update_mask(None, None, None) == 1
     assert L.mk_volume_set_transfer_function(None, 0, None, 0) == 1
     assert L.mk_volume_set_label_params(None, None, 1) == 1
     assert L.mk_volume_destroy(None) == 1
